@@ -1,0 +1,79 @@
+// Device-side parameter block, status word and small helpers shared by the
+// kernels of the single-partition step.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/icempm_b200.h"
+
+namespace icempm {
+
+// The subset of SimParams3D the kernels read, with derived constants, passed
+// by value as a kernel argument (the reference copies the whole struct to a
+// __constant__ symbol, gpu_partition_3d.cu:306; a by-value argument lives in
+// the same constant bank and keeps handles independent).
+struct DevParams {
+    int Gx, Gy, Gz, halo;          // GridXTotal, GridY, GridZ, GridHaloSize
+    int setup_type;
+    int subdiv;                    // IndenterSubdivisions
+    long long nodes;               // (Gx + 2 halo) * Gy * Gz
+    long long gstride;             // doubles between the 4 grid arrays
+    long long slab;                // Gy * Gz
+    double h, h_inv, dt;
+    double particle_mass, liquid_mass;
+    double dt_vol_Dpinv;
+    double dt_gravity, vmax, vmax_sq;
+    double ind_rsq, ind_velocity;
+    double mu, kappa;
+    double pmax, tensile, shear, tensile2, beta, grain_var;
+    double tan_phi, p0;            // DP_tan_phi, DP_threshold_p
+    double drag;
+};
+
+constexpr double kCoeff1 = 1.224744871391589;      // sqrt(3/2)
+constexpr double kCoeff1Inv = 0.8164965809277260;  // 1/sqrt(3/2)
+constexpr long long kCrushed = MPM_STATUS_CRUSHED;
+constexpr long long kDisabled = MPM_STATUS_DISABLED;
+constexpr long long kLiquid = MPM_STATUS_LIQUID;
+
+// First error wins (the reference's byte is overwritten by any failing
+// thread; with one failing particle the outcome is the same).
+__device__ __forceinline__ void raise_error(int* err, int code) {
+    if (*(volatile int*)err == 0) atomicCAS(err, 0, code);
+}
+
+// Bounds test of mpm_kernels.cuh:70-75 (one partition): the last failing
+// test of the sequence determines the code.
+__device__ __forceinline__ int stencil_error(const DevParams& P, int bx, int by, int bz) {
+    int e = 0;
+    if (bx < -P.halo) e = 70;
+    if (by < 0) e = 71;
+    if (bz < 0) e = 72;
+    if (bx > P.Gx + P.halo - 3) e = 73;
+    if (by > P.Gy - 3) e = 74;
+    if (bz > P.Gz - 3) e = 75;
+    return e;
+}
+
+__device__ __forceinline__ bool node_inside(const DevParams& P, int x, int y, int z) {
+    return x >= -P.halo && x < P.Gx + P.halo && y >= 0 && y < P.Gy && z >= 0 && z < P.Gz;
+}
+
+__device__ __forceinline__ long long node_index(const DevParams& P, int x, int y, int z) {
+    return ((long long)(x + P.halo) * P.Gy + y) * P.Gz + z;
+}
+
+template <typename T>
+__device__ __forceinline__ void quad_weights(const T fx[3], T ww[3][3]) {
+    // quadratic B-spline weights, mpm_kernels.cuh:78-81
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        T v0 = (T)1.5 - fx[d], v1 = fx[d] - (T)1.0, v2 = fx[d] - (T)0.5;
+        ww[0][d] = (T)0.5 * v0 * v0;
+        ww[1][d] = (T)0.75 - v1 * v1;
+        ww[2][d] = (T)0.5 * v2 * v2;
+    }
+}
+
+}  // namespace icempm

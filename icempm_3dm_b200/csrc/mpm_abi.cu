@@ -1,0 +1,638 @@
+// C-ABI of the single-partition MLS-MPM step (declared in include/icempm_b200.h).
+//
+// One handle = one partition on one device: particle SoA, grid, sensor array
+// and scratch, all on one stream. The substep sequence and the bookkeeping of
+// SimulationTime / SimulationStep follow Model3D::Step (model_3d.cpp:35-51)
+// and GPU_Implementation6 (gpu_implementation6.cpp); the kernels are in the
+// kernels_*.cuh / sort.cuh headers.
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/icempm_b200.h"
+#include "../../include/icempm_b200_testing.h"
+#include "device_common.cuh"
+#include "kernels_f64.cuh"
+#include "sort.cuh"
+
+using namespace icempm;
+
+struct mpm_handle {
+    SimParams3D prms;
+    DevParams dp;
+    int precision = MPM_PRECISION_FP64;
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    unsigned capacity = 0;
+    unsigned n = 0;
+    size_t pitch = 0;                 // doubles per SoA row on the device
+    bool uploaded = false;
+
+    double* pts = nullptr;            // 28 rows x pitch
+    double* p0 = nullptr;             // per-particle apex shift (optional)
+    unsigned* ids = nullptr;          // upload index of each particle
+    double* grid = nullptr;           // AoS {m, mv} per node
+    double* sensor = nullptr;         // 3 * subdiv * Gz
+    double* force_steps = nullptr;    // 3 per substep of the running mpm_step
+    int force_steps_cap = 0;
+    double* force_phase = nullptr;    // 3, substep force of the phase API
+    int* err = nullptr;
+
+    // sort scratch (allocated on first sort)
+    double* pts_alt = nullptr;
+    double* p0_alt = nullptr;
+    unsigned* ids_alt = nullptr;
+    int* s_bucket = nullptr;
+    int* s_count = nullptr;
+    int* s_start = nullptr;
+    unsigned* s_perm = nullptr;
+    std::vector<int*> scan_levels;    // per-level tile sums and their scans
+    std::vector<int> scan_sizes;
+    int sort_interval = 0;
+    int steps_since_sort = 0;
+
+    int p2g_variant = 0;              // 0 tile (default), 1 direct atomics
+    int tile_cap = 2048;              // P2G tile nodes (x 32 B of shared memory)
+    cudaError_t last_cuda = cudaSuccess;
+};
+
+namespace {
+
+thread_local char g_last_error[256] = "";
+
+int cuda_fail(mpm_handle* h, cudaError_t e, const char* what) {
+    if (h) h->last_cuda = e;
+    std::snprintf(g_last_error, sizeof(g_last_error), "%s: %s", what, cudaGetErrorString(e));
+    return MPM_ERR_CUDA;
+}
+
+#define CK(h, call)                                              \
+    do {                                                         \
+        cudaError_t e_ = (call);                                 \
+        if (e_ != cudaSuccess) return cuda_fail((h), e_, #call); \
+    } while (0)
+
+#define CK_LAUNCH(h, what)                                      \
+    do {                                                        \
+        cudaError_t e_ = cudaGetLastError();                    \
+        if (e_ != cudaSuccess) return cuda_fail((h), e_, what); \
+    } while (0)
+
+DevParams make_dev_params(const SimParams3D& p) {
+    DevParams d;
+    std::memset(&d, 0, sizeof(d));
+    d.Gx = p.GridXTotal;
+    d.Gy = p.GridY;
+    d.Gz = p.GridZ;
+    d.halo = p.GridHaloSize;
+    d.setup_type = p.SetupType;
+    d.subdiv = p.IndenterSubdivisions;
+    d.slab = (long long)p.GridY * p.GridZ;
+    d.nodes = (long long)(p.GridXTotal + 2 * p.GridHaloSize) * d.slab;
+    d.gstride = (d.nodes + 31) / 32 * 32;
+    d.h = p.cellsize;
+    d.h_inv = p.cellsize_inv;
+    d.dt = p.InitialTimeStep;
+    d.particle_mass = p.ParticleMass;
+    d.liquid_mass = p.LiquidParticleMass;
+    d.dt_vol_Dpinv = p.dt_vol_Dpinv;
+    d.dt_gravity = p.dt_Gravity;
+    d.vmax = p.vmax;
+    d.vmax_sq = p.vmax_squared;
+    d.ind_rsq = p.IndRSq;
+    d.ind_velocity = p.IndVelocity;
+    d.mu = p.mu;
+    d.kappa = p.kappa;
+    d.pmax = p.IceCompressiveStrength;
+    d.tensile = p.IceTensileStrength;
+    d.shear = p.IceShearStrength;
+    d.tensile2 = p.IceTensileStrength2;
+    d.beta = p.NACC_beta;
+    d.grain_var = p.GrainVariability;
+    d.tan_phi = p.DP_tan_phi;
+    d.p0 = p.DP_threshold_p;
+    d.drag = p.DragGlobal;
+    return d;
+}
+
+bool params_valid(const SimParams3D* p) {
+    return p && p->GridXTotal > 0 && p->GridY > 0 && p->GridZ > 0 && p->GridHaloSize >= 0 && p->cellsize > 0 &&
+           p->InitialTimeStep > 0 && p->IndenterSubdivisions > 0 && p->UpdateEveryNthStep > 0;
+}
+
+inline unsigned blocks_for(long long n, int tpb) { return (unsigned)((n + tpb - 1) / tpb); }
+
+void free_all(mpm_handle* h) {
+    cudaFree(h->pts); cudaFree(h->p0); cudaFree(h->ids); cudaFree(h->grid); cudaFree(h->sensor);
+    cudaFree(h->force_steps); cudaFree(h->force_phase); cudaFree(h->err);
+    cudaFree(h->pts_alt); cudaFree(h->p0_alt); cudaFree(h->ids_alt);
+    cudaFree(h->s_bucket); cudaFree(h->s_count); cudaFree(h->s_start); cudaFree(h->s_perm);
+    for (int* p : h->scan_levels) cudaFree(p);
+    h->scan_levels.clear();
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+}
+
+size_t sensor_count(const SimParams3D& p) { return (size_t)3 * p.IndenterSubdivisions * p.GridZ; }
+
+// ---------------------------------------------------------------- phases
+
+int launch_p2g(mpm_handle* h) {
+    const int n = (int)h->n;
+    if (n == 0) return MPM_OK;
+    const size_t smem = sizeof(double) * 4 * h->tile_cap;
+    switch (h->p2g_variant) {
+        case 1:
+            k_p2g_direct_f64<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, h->err);
+            break;
+        case 2:
+            k_p2g_warpagg_f64<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, h->err);
+            break;
+        case 3:
+            k_p2g_tile_f64<256, true><<<blocks_for(n, 256), 256, smem, h->stream>>>(h->dp, h->pts, h->pitch, n,
+                                                                                     h->grid, h->err, h->tile_cap);
+            break;
+        default:
+            k_p2g_tile_f64<256, false><<<blocks_for(n, 256), 256, smem, h->stream>>>(h->dp, h->pts, h->pitch, n,
+                                                                                      h->grid, h->err, h->tile_cap);
+            break;
+    }
+    CK_LAUNCH(h, "p2g kernel");
+    return MPM_OK;
+}
+
+int launch_update(mpm_handle* h, double ind_x, double ind_y, double* force3) {
+    k_update_f64<256><<<blocks_for(h->dp.nodes, 256), 256, 0, h->stream>>>(h->dp, h->grid, ind_x, ind_y, h->sensor,
+                                                                             force3);
+    CK_LAUNCH(h, "update kernel");
+    return MPM_OK;
+}
+
+int launch_g2p(mpm_handle* h, int record_pq) {
+    const int n = (int)h->n;
+    if (n == 0) return MPM_OK;
+    if (h->precision == MPM_PRECISION_FP64) {
+        k_g2p_f64<SvdF32><<<blocks_for(n, 128), 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, record_pq,
+                                                                      h->p0, h->err);
+    } else {
+        k_g2p_f64<SvdF64><<<blocks_for(n, 128), 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, record_pq,
+                                                                      h->p0, h->err);
+    }
+    CK_LAUNCH(h, "g2p kernel");
+    return MPM_OK;
+}
+
+int reset_grid(mpm_handle* h) {
+    CK(h, cudaMemsetAsync(h->grid, 0, sizeof(double) * 4 * (size_t)h->dp.gstride, h->stream));
+    return MPM_OK;
+}
+
+int read_error(mpm_handle* h, int* code) {
+    CK(h, cudaMemcpyAsync(code, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+}
+
+// ------------------------------------------------------------------ sort
+
+int ensure_sort_scratch(mpm_handle* h) {
+    if (h->s_bucket) return MPM_OK;
+    const SimParams3D& p = h->prms;
+    const long long nb = (long long)(p.GridXTotal + 2 * p.GridHaloSize + 1) * p.GridY * p.GridZ;
+    if (nb + 1 > 0x7fffffffLL) return MPM_ERR_ARG;
+    CK(h, cudaMalloc(&h->pts_alt, sizeof(double) * MPM_N_PTS_ARRAYS * h->pitch));
+    CK(h, cudaMalloc(&h->ids_alt, sizeof(unsigned) * h->pitch));
+    CK(h, cudaMalloc(&h->s_bucket, sizeof(int) * h->pitch));
+    CK(h, cudaMalloc(&h->s_perm, sizeof(unsigned) * h->pitch));
+    CK(h, cudaMalloc(&h->s_count, sizeof(int) * (nb + 1)));
+    CK(h, cudaMalloc(&h->s_start, sizeof(int) * (nb + 1)));
+    long long m = nb + 1;
+    while (m > kScanTile) {
+        m = (m + kScanTile - 1) / kScanTile;
+        int* sums = nullptr;
+        int* scanned = nullptr;
+        CK(h, cudaMalloc(&sums, sizeof(int) * m));
+        CK(h, cudaMalloc(&scanned, sizeof(int) * m));
+        h->scan_levels.push_back(sums);
+        h->scan_levels.push_back(scanned);
+        h->scan_sizes.push_back((int)m);
+    }
+    return MPM_OK;
+}
+
+int exclusive_scan(mpm_handle* h, const int* in, int* out, int n, size_t level) {
+    const int tiles = (n + kScanTile - 1) / kScanTile;
+    int* sums = tiles > 1 ? h->scan_levels[2 * level] : nullptr;
+    k_scan_tiles<<<tiles, kScanBlock, 0, h->stream>>>(in, out, n, sums);
+    CK_LAUNCH(h, "scan tiles");
+    if (tiles > 1) {
+        int* scanned = h->scan_levels[2 * level + 1];
+        int r = exclusive_scan(h, sums, scanned, tiles, level + 1);
+        if (r) return r;
+        k_scan_add<<<blocks_for(n, 256), 256, 0, h->stream>>>(out, n, scanned);
+        CK_LAUNCH(h, "scan add");
+    }
+    return MPM_OK;
+}
+
+int do_sort(mpm_handle* h) {
+    if (h->n == 0) return MPM_OK;
+    int r = ensure_sort_scratch(h);
+    if (r) return r;
+    const SimParams3D& p = h->prms;
+    SortGeom G;
+    G.slab = p.GridY * p.GridZ;
+    G.gz = p.GridZ;
+    G.key_shift = p.GridHaloSize * G.slab;
+    G.nb = (p.GridXTotal + 2 * p.GridHaloSize + 1) * G.slab;
+    G.h_inv = p.cellsize_inv;
+    const int n = (int)h->n;
+    const int nb1 = G.nb + 1;
+    CK(h, cudaMemsetAsync(h->s_count, 0, sizeof(int) * nb1, h->stream));
+    k_sort_keys<<<blocks_for(n, 256), 256, 0, h->stream>>>(G, h->pts, h->pitch, n, h->s_bucket, h->s_count, h->err);
+    CK_LAUNCH(h, "sort keys");
+    r = exclusive_scan(h, h->s_count, h->s_start, nb1, 0);
+    if (r) return r;
+    CK(h, cudaMemsetAsync(h->s_count, 0, sizeof(int) * nb1, h->stream));
+    k_sort_scatter<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->s_bucket, n, h->s_start, h->s_count, h->s_perm);
+    CK_LAUNCH(h, "sort scatter");
+    k_sort_fix<<<blocks_for(G.nb, 256), 256, 0, h->stream>>>(G.nb, h->s_start, h->s_count, h->s_perm);
+    CK_LAUNCH(h, "sort fix");
+    int kept = 0;
+    CK(h, cudaMemcpyAsync(&kept, h->s_start + G.nb, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (kept > 0) {
+        dim3 grid(blocks_for(kept, 256), MPM_N_PTS_ARRAYS);
+        k_gather_rows<double><<<grid, 256, 0, h->stream>>>(h->pts, h->pitch, h->pts_alt, h->pitch, MPM_N_PTS_ARRAYS,
+                                                           h->s_perm, kept);
+        CK_LAUNCH(h, "gather rows");
+        k_gather_rows<unsigned><<<dim3(blocks_for(kept, 256), 1), 256, 0, h->stream>>>(h->ids, h->pitch, h->ids_alt,
+                                                                                       h->pitch, 1, h->s_perm, kept);
+        CK_LAUNCH(h, "gather ids");
+        if (h->p0) {
+            if (!h->p0_alt) CK(h, cudaMalloc(&h->p0_alt, sizeof(double) * h->pitch));
+            k_gather_rows<double><<<dim3(blocks_for(kept, 256), 1), 256, 0, h->stream>>>(h->p0, h->pitch, h->p0_alt,
+                                                                                         h->pitch, 1, h->s_perm, kept);
+            CK_LAUNCH(h, "gather p0");
+            std::swap(h->p0, h->p0_alt);
+        }
+        std::swap(h->pts, h->pts_alt);
+        std::swap(h->ids, h->ids_alt);
+    }
+    h->n = (unsigned)kept;
+    h->steps_since_sort = 0;
+    return MPM_OK;
+}
+
+}  // namespace
+
+// ==================================================================== ABI
+
+extern "C" {
+
+mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity, int device, int* status) {
+    int st = MPM_OK;
+    mpm_handle* h = nullptr;
+    do {
+        if (!params_valid(prms) || capacity == 0 ||
+            (precision != MPM_PRECISION_FP64 && precision != MPM_PRECISION_FP64_SVD64)) {
+            st = MPM_ERR_ARG;
+            break;
+        }
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0 || device < 0 || device >= count) {
+            cudaGetLastError();
+            st = MPM_ERR_NO_DEVICE;
+            break;
+        }
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) {
+            st = MPM_ERR_NO_DEVICE;
+            break;
+        }
+        h = new (std::nothrow) mpm_handle();
+        if (!h) { st = MPM_ERR_ARG; break; }
+        h->prms = *prms;
+        h->dp = make_dev_params(*prms);
+        h->precision = precision;
+        h->device = device;
+        h->capacity = capacity;
+        h->pitch = ((size_t)capacity + 31) / 32 * 32;
+        if (cudaSetDevice(device) != cudaSuccess) { st = MPM_ERR_CUDA; break; }
+        if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) { st = MPM_ERR_CUDA; break; }
+        h->stream = h->own_stream;
+        if (cudaFuncSetAttribute(k_p2g_tile_f64<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(double) * 4 * h->tile_cap)) != cudaSuccess ||
+            cudaFuncSetAttribute(k_p2g_tile_f64<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(double) * 4 * h->tile_cap)) != cudaSuccess) {
+            st = MPM_ERR_CUDA;
+            break;
+        }
+        const size_t ns = sensor_count(*prms);
+        if (cudaMalloc(&h->pts, sizeof(double) * MPM_N_PTS_ARRAYS * h->pitch) != cudaSuccess ||
+            cudaMalloc(&h->ids, sizeof(unsigned) * h->pitch) != cudaSuccess ||
+            cudaMalloc(&h->grid, sizeof(double) * 4 * (size_t)h->dp.gstride) != cudaSuccess ||
+            cudaMalloc(&h->sensor, sizeof(double) * ns) != cudaSuccess ||
+            cudaMalloc(&h->force_phase, sizeof(double) * 3) != cudaSuccess ||
+            cudaMalloc(&h->err, sizeof(int)) != cudaSuccess) {
+            st = MPM_ERR_CUDA;
+            break;
+        }
+        cudaMemsetAsync(h->pts, 0, sizeof(double) * MPM_N_PTS_ARRAYS * h->pitch, h->stream);
+        cudaMemsetAsync(h->grid, 0, sizeof(double) * 4 * (size_t)h->dp.gstride, h->stream);
+        cudaMemsetAsync(h->sensor, 0, sizeof(double) * ns, h->stream);
+        cudaMemsetAsync(h->force_phase, 0, sizeof(double) * 3, h->stream);
+        cudaMemsetAsync(h->err, 0, sizeof(int), h->stream);
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess) { st = MPM_ERR_CUDA; break; }
+    } while (0);
+    if (status) *status = st;
+    if (st != MPM_OK) {
+        if (h) { free_all(h); delete h; }
+        return nullptr;
+    }
+    return h;
+}
+
+void mpm_destroy(mpm_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+}
+
+int mpm_set_stream(mpm_handle* h, void* s) {
+    if (!h) return MPM_ERR_ARG;
+    CK(h, cudaStreamSynchronize(h->stream));
+    h->stream = s ? (cudaStream_t)s : h->own_stream;
+    return MPM_OK;
+}
+
+int mpm_update_constants(mpm_handle* h, const SimParams3D* prms) {
+    if (!h || !params_valid(prms)) return MPM_ERR_ARG;
+    if (prms->GridXTotal != h->prms.GridXTotal || prms->GridY != h->prms.GridY || prms->GridZ != h->prms.GridZ ||
+        prms->GridHaloSize != h->prms.GridHaloSize || prms->IndenterSubdivisions != h->prms.IndenterSubdivisions)
+        return MPM_ERR_ARG;
+    h->prms = *prms;
+    h->dp = make_dev_params(*prms);
+    CK(h, cudaMemsetAsync(h->err, 0, sizeof(int), h->stream));
+    return MPM_OK;
+}
+
+int mpm_upload_soa(mpm_handle* h, const double* soa, unsigned pitch, unsigned n) {
+    if (!h || (!soa && n) || pitch < n) return MPM_ERR_ARG;
+    if (n > h->capacity) return MPM_ERR_CAPACITY;
+    if (n) {
+        CK(h, cudaMemcpy2DAsync(h->pts, sizeof(double) * h->pitch, soa, sizeof(double) * pitch, sizeof(double) * n,
+                                MPM_N_PTS_ARRAYS, cudaMemcpyHostToDevice, h->stream));
+        std::vector<unsigned> ids(n);
+        for (unsigned i = 0; i < n; i++) ids[i] = i;
+        CK(h, cudaMemcpyAsync(h->ids, ids.data(), sizeof(unsigned) * n, cudaMemcpyHostToDevice, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+    }
+    h->n = n;
+    h->uploaded = true;
+    CK(h, cudaMemsetAsync(h->err, 0, sizeof(int), h->stream));
+    return MPM_OK;
+}
+
+int mpm_upload_cohesion(mpm_handle* h, const double* c, unsigned n) {
+    if (!h) return MPM_ERR_ARG;
+    if (!c) {
+        cudaFree(h->p0);
+        cudaFree(h->p0_alt);
+        h->p0 = h->p0_alt = nullptr;
+        return MPM_OK;
+    }
+    if (n != h->n || h->prms.DP_tan_phi == 0) return MPM_ERR_ARG;
+    if (!h->p0) CK(h, cudaMalloc(&h->p0, sizeof(double) * h->pitch));
+    std::vector<double> p0(n);
+    for (unsigned i = 0; i < n; i++) p0[i] = c[i] / h->prms.DP_tan_phi;
+    CK(h, cudaMemcpyAsync(h->p0, p0.data(), sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+}
+
+int mpm_download_soa(mpm_handle* h, double* soa, unsigned pitch, unsigned* n) {
+    if (!h || !soa || pitch < h->n) return MPM_ERR_ARG;
+    if (h->n) {
+        CK(h, cudaMemcpy2DAsync(soa, sizeof(double) * pitch, h->pts, sizeof(double) * h->pitch, sizeof(double) * h->n,
+                                MPM_N_PTS_ARRAYS, cudaMemcpyDeviceToHost, h->stream));
+    }
+    int code = 0;
+    int r = read_error(h, &code);
+    if (r) return r;
+    if (n) *n = h->n;
+    return code;
+}
+
+int mpm_download_ids(mpm_handle* h, unsigned* ids, unsigned* n) {
+    if (!h || !ids) return MPM_ERR_ARG;
+    if (h->n) CK(h, cudaMemcpyAsync(ids, h->ids, sizeof(unsigned) * h->n, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (n) *n = h->n;
+    return MPM_OK;
+}
+
+int mpm_sort(mpm_handle* h) {
+    if (!h) return MPM_ERR_ARG;
+    if (!h->uploaded) return MPM_ERR_STATE;
+    int r = do_sort(h);
+    if (r) return r;
+    int code = 0;
+    r = read_error(h, &code);
+    return r ? r : code;
+}
+
+int mpm_set_sort_interval(mpm_handle* h, int k) {
+    if (!h || k < 0) return MPM_ERR_ARG;
+    h->sort_interval = k;
+    return MPM_OK;
+}
+
+int mpm_reset_grid(mpm_handle* h) {
+    if (!h) return MPM_ERR_ARG;
+    return reset_grid(h);
+}
+
+int mpm_p2g(mpm_handle* h) {
+    if (!h) return MPM_ERR_ARG;
+    if (!h->uploaded) return MPM_ERR_STATE;
+    return launch_p2g(h);
+}
+
+int mpm_update_nodes(mpm_handle* h, double indenter_x, double indenter_y) {
+    if (!h) return MPM_ERR_ARG;
+    return launch_update(h, indenter_x, indenter_y, h->force_phase);
+}
+
+int mpm_g2p(mpm_handle* h, int record_pq) {
+    if (!h) return MPM_ERR_ARG;
+    if (!h->uploaded) return MPM_ERR_STATE;
+    return launch_g2p(h, record_pq);
+}
+
+int mpm_reset_indenter_force_accumulator(mpm_handle* h) {
+    if (!h) return MPM_ERR_ARG;
+    CK(h, cudaMemsetAsync(h->sensor, 0, sizeof(double) * sensor_count(h->prms), h->stream));
+    return MPM_OK;
+}
+
+int mpm_step(mpm_handle* h, int nsteps, double* force_hist) {
+    if (!h || nsteps < 0) return MPM_ERR_ARG;
+    if (!h->uploaded) return MPM_ERR_STATE;
+    if (nsteps == 0) return MPM_OK;
+    if (nsteps > h->force_steps_cap) {
+        CK(h, cudaStreamSynchronize(h->stream));
+        cudaFree(h->force_steps);
+        h->force_steps = nullptr;
+        CK(h, cudaMalloc(&h->force_steps, sizeof(double) * 3 * (size_t)nsteps));
+        h->force_steps_cap = nsteps;
+    }
+    CK(h, cudaMemsetAsync(h->force_steps, 0, sizeof(double) * 3 * (size_t)nsteps, h->stream));
+    SimParams3D& p = h->prms;
+    for (int s = 0; s < nsteps; s++) {
+        p.SimulationTime += p.InitialTimeStep;
+        p.indenter_x = p.indenter_x_initial + p.SimulationTime * p.IndVelocity;
+        int r;
+        if ((r = reset_grid(h))) return r;
+        if ((r = launch_p2g(h))) return r;
+        if ((r = launch_update(h, p.indenter_x, p.indenter_y, h->force_steps + 3 * s))) return r;
+        const int record = (p.SimulationStep % p.UpdateEveryNthStep) == 0;
+        if ((r = launch_g2p(h, record))) return r;
+        p.SimulationStep += 1;
+        if (h->sort_interval > 0 && ++h->steps_since_sort >= h->sort_interval) {
+            if ((r = do_sort(h))) return r;
+        }
+    }
+    if (force_hist) {
+        CK(h, cudaMemcpyAsync(force_hist, h->force_steps, sizeof(double) * 3 * (size_t)nsteps, cudaMemcpyDeviceToHost,
+                              h->stream));
+    }
+    int code = 0;
+    int r = read_error(h, &code);
+    return r ? r : code;
+}
+
+int mpm_sensors(mpm_handle* h, double* sensor, double total[3]) {
+    if (!h) return MPM_ERR_ARG;
+    const size_t ns = sensor_count(h->prms);
+    std::vector<double> s(ns);
+    CK(h, cudaMemcpyAsync(s.data(), h->sensor, sizeof(double) * ns, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    const SimParams3D& p = h->prms;
+    double t[3] = {0, 0, 0};
+    for (size_t j = 0; j < ns / 3; j++)
+        for (int k = 0; k < 3; k++) t[k] += s[3 * j + k];
+    for (int k = 0; k < 3; k++) t[k] /= (double)p.UpdateEveryNthStep;
+    const double norm = (double)(p.UpdateEveryNthStep * p.cellsize * p.cellsize);
+    if (sensor)
+        for (size_t j = 0; j < ns; j++) sensor[j] = s[j] / norm;
+    if (total)
+        for (int k = 0; k < 3; k++) total[k] = t[k];
+    return MPM_OK;
+}
+
+int mpm_get_error(mpm_handle* h) {
+    if (!h) return MPM_ERR_ARG;
+    int code = 0;
+    int r = read_error(h, &code);
+    return r ? r : code;
+}
+
+int mpm_synchronize(mpm_handle* h) {
+    if (!h) return MPM_ERR_ARG;
+    CK(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+}
+
+int mpm_get_params(mpm_handle* h, SimParams3D* out) {
+    if (!h || !out) return MPM_ERR_ARG;
+    *out = h->prms;
+    return MPM_OK;
+}
+
+int mpm_count(mpm_handle* h, unsigned* n) {
+    if (!h || !n) return MPM_ERR_ARG;
+    *n = h->n;
+    return MPM_OK;
+}
+
+const char* mpm_last_error_string(void) { return g_last_error; }
+
+}  // extern "C"
+
+// ------------------------------------------------------------ test hooks
+
+namespace {
+template <class K>
+__global__ void k_svd_batch(const double* __restrict__ A, int count, double* __restrict__ U, double* __restrict__ S,
+                            double* __restrict__ V) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    typedef typename K::T T;
+    T a[3][3], u[3][3], s[3], v[3][3];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) a[r][c] = (T)A[9 * i + 3 * r + c];
+    svd3x3<K>(a, u, s, v);
+    for (int r = 0; r < 3; r++) {
+        S[3 * i + r] = (double)s[r];
+        for (int c = 0; c < 3; c++) {
+            U[9 * i + 3 * r + c] = (double)u[r][c];
+            V[9 * i + 3 * r + c] = (double)v[r][c];
+        }
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int mpm_testing_svd3x3(int mode, const double* A, int count, double* U, double* S, double* V, int device) {
+    if (!A || !U || !S || !V || count <= 0 || (mode != 0 && mode != 1)) return MPM_ERR_ARG;
+    CK(nullptr, cudaSetDevice(device));
+    double *dA = nullptr, *dU = nullptr, *dS = nullptr, *dV = nullptr;
+    const size_t m9 = sizeof(double) * 9 * (size_t)count, m3 = sizeof(double) * 3 * (size_t)count;
+    int st = MPM_OK;
+    if (cudaMalloc(&dA, m9) != cudaSuccess || cudaMalloc(&dU, m9) != cudaSuccess ||
+        cudaMalloc(&dS, m3) != cudaSuccess || cudaMalloc(&dV, m9) != cudaSuccess) {
+        st = cuda_fail(nullptr, cudaGetLastError(), "svd scratch");
+    } else {
+        cudaMemcpy(dA, A, m9, cudaMemcpyHostToDevice);
+        if (mode == 0) k_svd_batch<SvdF32><<<blocks_for(count, 128), 128>>>(dA, count, dU, dS, dV);
+        else k_svd_batch<SvdF64><<<blocks_for(count, 128), 128>>>(dA, count, dU, dS, dV);
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) st = cuda_fail(nullptr, e, "svd kernel");
+        else {
+            cudaMemcpy(U, dU, m9, cudaMemcpyDeviceToHost);
+            cudaMemcpy(S, dS, m3, cudaMemcpyDeviceToHost);
+            cudaMemcpy(V, dV, m9, cudaMemcpyDeviceToHost);
+        }
+    }
+    cudaFree(dA); cudaFree(dU); cudaFree(dS); cudaFree(dV);
+    return st;
+}
+
+size_t mpm_testing_sizeof_params(void) { return sizeof(SimParams3D); }
+
+int mpm_testing_download_grid(mpm_handle* h, double* out) {
+    if (!h || !out) return MPM_ERR_ARG;
+    const size_t nodes = (size_t)h->dp.nodes;
+    for (int c = 0; c < 4; c++)
+        CK(h, cudaMemcpyAsync(out + c * nodes, h->grid + c * h->dp.gstride, sizeof(double) * nodes,
+                              cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+}
+
+int mpm_testing_set_p2g_variant(mpm_handle* h, int variant) {
+    if (!h || variant < 0 || variant > 3) return MPM_ERR_ARG;
+    h->p2g_variant = variant;
+    return MPM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,212 @@
+"""Seeded synthetic ice blocks for the indentation setup.
+
+The reference reads gmsh/Poisson-disk point clouds from HDF5
+(SnapshotManager::LoadRawPoints, snapshotmanager.cpp:20-113). This module
+generates a stand-in with the shapes and sizes of the benchmark workloads:
+a jittered cubic lattice, seeded by a counter-based RNG (splitmix64, keyed by
+seed, particle index and stream), then placed and initialised exactly as
+LoadRawPoints does:
+  - block offset: x centred in the domain, lowest point at y = 2h, z centred
+    (snapshotmanager.cpp:57-75);
+  - F = I, Jp_inv = 1 (HostSideSOA::InitializeBlock, host_side_soa.cpp:88-97);
+  - indenter start x = floor((block_left - sqrt(r^2 - (r-IndDepth)^2))/h) h,
+    y = block_top + r - IndDepth (snapshotmanager.cpp:82-96);
+  - ParticleVolume = Volume / N (:99).
+Per-particle cohesion (lognormal) is drawn from the same RNG.
+"""
+import dataclasses
+import math
+
+import numpy as np
+
+from ._lib import (BP00, FE00, IDX_JP_INV, LIB, N_PTS_ARRAYS, POSX, SimParams3D)
+
+_M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def splitmix64(x):
+    """splitmix64 finaliser (Steele, Lea, Flood 2014), vectorised on uint64."""
+    x = np.asarray(x, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = x + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def uniform(seed, idx, stream):
+    """Uniform doubles in [0, 1) for particle indices idx (counter-based)."""
+    idx = np.asarray(idx, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        key = splitmix64(np.uint64(seed) * np.uint64(0x632BE59BD9B4E019) + np.uint64(stream))
+        r = splitmix64(key ^ (idx * np.uint64(0xD1B54A32D192ED03)))
+    return (r >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def normal(seed, idx, stream):
+    """Standard normal deviates by Box-Muller on two uniform streams."""
+    u1 = uniform(seed, idx, 2 * stream + 1000)
+    u2 = uniform(seed, idx, 2 * stream + 1001)
+    u1 = np.maximum(u1, 1e-300)
+    return np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * math.pi * u2)
+
+
+def jittered_lattice(n, dims, seed, jitter=0.3):
+    """n points in the box [0, dims] on a jittered cubic lattice.
+
+    Spacing s = (V/n)^(1/3); per-axis counts ceil(L/s) (spacing adjusted to
+    fill the box); if the lattice holds more than n sites, a seeded subset of
+    n sites is kept in lattice order (x slowest, z fastest). Each coordinate
+    moves by a uniform +-jitter * spacing.
+    """
+    L = np.asarray(dims, dtype=np.float64)
+    s = (L.prod() / n) ** (1.0 / 3.0)
+    counts = np.maximum(1, np.ceil(L / s - 1e-9).astype(np.int64))
+    total = int(counts.prod())
+    if total < n:
+        raise ValueError("lattice smaller than n")
+    sites = np.arange(total, dtype=np.int64)
+    if total > n:
+        u = uniform(seed, sites, 7)
+        keep = np.argpartition(u, n)[:n]
+        sites = np.sort(keep)
+    nz, ny = counts[2], counts[1]
+    ix = sites // (ny * nz)
+    iy = (sites // nz) % ny
+    iz = sites % nz
+    sp = L / counts
+    pid = np.arange(n, dtype=np.uint64)
+    pos = np.empty((3, n))
+    for d, ii in enumerate((ix, iy, iz)):
+        j = (2.0 * uniform(seed, pid, d) - 1.0) * jitter
+        pos[d] = (ii + 0.5 + j) * sp[d]
+    return pos
+
+
+@dataclasses.dataclass
+class BlockConfig:
+    """One indentation workload (block on a sticky floor, cylinder moving +x)."""
+    name: str
+    n: int
+    dims: tuple
+    h: float
+    seed: int
+    dt: float
+    steps: int
+    ind_velocity: float
+    cohesion_median: float = 3.0e5
+    cohesion_sigma_log: float = 0.0          # 0: uniform cohesion
+    density: float = 917.0
+    youngs: float = 5.0e8
+    poisson: float = 0.3
+    phi_deg: float = 62.0
+    ind_radius: float = 0.05
+    pad: int = 3                              # wall pad nodes per side
+    halo: int = 0                             # GridHaloSize (one partition)
+
+
+CONFIGS = {
+    "block250k": BlockConfig("block250k", 250_000, (1.0, 0.5, 0.5), 0.01, 0, 1e-5, 1000, 0.2),
+    "block2m": BlockConfig("block2m", 2_000_000, (2.0, 1.0, 1.0), 0.0125, 1, 5e-6, 2000, 0.5,
+                           cohesion_sigma_log=0.3),
+    "block8m": BlockConfig("block8m", 8_000_000, (4.0, 1.0, 1.0), 0.01, 2, 5e-6, 2000, 1.0,
+                           cohesion_sigma_log=0.3),
+    "calib500k": BlockConfig("calib500k", 500_000, (1.0, 0.5, 0.5), 0.01, 3, 1e-5, 200, 0.2),
+}
+
+
+def grid_dims(cfg):
+    """Nodes: block cells + wall pads; in x also room for the indenter on the
+    -x side (centred block, as LoadRawPoints centres it); in y the block
+    stands 2h above the floor."""
+    nb = [int(math.ceil(L / cfg.h - 1e-9)) for L in cfg.dims]
+    clear = int(math.ceil(cfg.ind_radius / cfg.h)) + 2
+    gx = nb[0] + 2 * (cfg.pad + clear)
+    gy = nb[1] + 2 + cfg.pad + 3
+    gz = nb[2] + 2 * cfg.pad + 2
+    return gx, gy, gz
+
+
+def make_params(cfg, n=None):
+    """SimParams3D for cfg; derived constants via the library's own
+    ComputeCamClayParams / ComputeHelperVariables."""
+    p = SimParams3D()
+    LIB.mpm_params_reset(p)
+    gx, gy, gz = grid_dims(cfg)
+    p.GridXTotal, p.GridY, p.GridZ = gx, gy, gz
+    p.DomainDimensionX = gx * cfg.h
+    p.GridHaloSize = cfg.halo
+    p.nPartitions = 1
+    p.InitialTimeStep = cfg.dt
+    p.YoungsModulus = cfg.youngs
+    p.PoissonsRatio = cfg.poisson
+    p.Density = cfg.density
+    LIB.mpm_params_set_phi(p, cfg.phi_deg)
+    p.DP_threshold_p = cfg.cohesion_median / p.DP_tan_phi
+    p.GrainVariability = 0.0
+    p.IndDiameter = 2 * cfg.ind_radius
+    p.IndVelocity = cfg.ind_velocity
+    p.IndDepth = cfg.ind_radius
+    p.nPtsTotal = cfg.n if n is None else n
+    p.Volume = float(np.prod(cfg.dims))
+    LIB.mpm_params_compute_camclay(p)
+    LIB.mpm_params_compute_helper_variables(p)
+    return p
+
+
+def make_block(cfg, n=None):
+    """(prms, soa, cohesion): soa is a (28, n) float64 host SoA in the
+    reference layout; cohesion is None for uniform cohesion."""
+    n = cfg.n if n is None else n
+    dims = cfg.dims
+    if n != cfg.n:   # a smaller copy of the same block keeps the spacing
+        scale = (n / cfg.n) ** (1.0 / 3.0)
+        dims = tuple(d * scale for d in cfg.dims)
+        cfg = dataclasses.replace(cfg, dims=dims, n=n)
+    p = make_params(cfg, n)
+    pos = jittered_lattice(n, dims, cfg.seed)
+    h = p.cellsize
+    mins, maxs = pos.min(axis=1), pos.max(axis=1)
+    box_x, box_z = p.GridXTotal * h, p.GridZ * h
+    x_off = (box_x - (maxs[0] - mins[0])) / 2
+    y_off = 2 * h - mins[1]
+    z_off = (box_z - (maxs[2] - mins[2])) / 2
+    pos[0] += x_off
+    pos[1] += y_off
+    pos[2] += z_off
+    p.xmin, p.ymin, p.zmin = mins
+    p.xmax, p.ymax, p.zmax = maxs
+    block_left = x_off
+    block_top = p.ymax + y_off
+    r = p.IndDiameter / 2
+    ht = r - p.IndDepth
+    x_ind_offset = math.sqrt(r * r - ht * ht)
+    p.indenter_x = math.floor((block_left - x_ind_offset) / h) * h
+    p.indenter_y = block_top + ht
+    p.indenter_x_initial = p.indenter_x
+    p.indenter_y_initial = p.indenter_y
+    p.ParticleVolume = p.Volume / n
+    LIB.mpm_params_compute_helper_variables(p)
+
+    soa = np.zeros((N_PTS_ARRAYS, n), dtype=np.float64)
+    soa[POSX:POSX + 3] = pos
+    soa[IDX_JP_INV] = 1.0
+    for i in range(3):
+        soa[FE00 + 4 * i] = 1.0
+    cohesion = None
+    if cfg.cohesion_sigma_log > 0:
+        z = normal(cfg.seed, np.arange(n, dtype=np.uint64), 11)
+        cohesion = cfg.cohesion_median * np.exp(cfg.cohesion_sigma_log * z)
+    return p, soa, cohesion
+
+
+def small_block(n=4000, seed=5, dims=(0.2, 0.1, 0.1), h=0.01, dt=1e-5, ind_velocity=0.2,
+                cohesion_sigma_log=0.0, youngs=5e8):
+    """A small block for parity tests (seconds on the oracle)."""
+    cfg = BlockConfig("small", n, dims, h, seed, dt, 0, ind_velocity, cohesion_sigma_log=cohesion_sigma_log,
+                      youngs=youngs)
+    return make_block(cfg)
+
+
+__all__ = ["BlockConfig", "CONFIGS", "make_block", "make_params", "small_block", "jittered_lattice",
+           "splitmix64", "uniform", "normal", "BP00"]

@@ -1,0 +1,240 @@
+"""Host-side mirror of the reference's step API over the C-ABI.
+
+  MPMHandle            one partition on one GPU (mpm_create ... mpm_destroy)
+  GPU_Implementation6  the reference class's method names and call order
+                       (simulation/gpu_implementation6.h:24-59) for one
+                       partition: halo and point-transfer methods are no-ops
+  Model3D              the substep loop of Model3D::Step (model_3d.cpp:24-112)
+
+All device work runs in the CUDA library; nothing here computes physics.
+"""
+import numpy as np
+
+from ._lib import (LIB, N_PTS_ARRAYS, PRECISION_FP64, MPMError, SimParams3D, check, dptr, uptr)
+import ctypes
+
+
+class MPMHandle:
+    def __init__(self, prms, capacity, precision=PRECISION_FP64, device=0):
+        st = ctypes.c_int(0)
+        self.prms = prms.copy()
+        self.precision = precision
+        self._h = LIB.mpm_create(ctypes.byref(self.prms), precision, int(capacity), device, ctypes.byref(st))
+        if not self._h:
+            raise MPMError(st.value, "mpm_create")
+        self.capacity = int(capacity)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            LIB.mpm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- data
+    def upload(self, soa, n=None, cohesion=None):
+        soa = np.ascontiguousarray(soa, dtype=np.float64)
+        assert soa.shape[0] == N_PTS_ARRAYS
+        n = soa.shape[1] if n is None else n
+        check(LIB.mpm_upload_soa(self._h, dptr(soa), soa.shape[1], n), "mpm_upload_soa")
+        if cohesion is not None:
+            c = np.ascontiguousarray(cohesion, dtype=np.float64)
+            check(LIB.mpm_upload_cohesion(self._h, dptr(c), n), "mpm_upload_cohesion")
+
+    def count(self):
+        n = ctypes.c_uint(0)
+        check(LIB.mpm_count(self._h, ctypes.byref(n)), "mpm_count")
+        return n.value
+
+    def download(self, raise_on_error=True):
+        n = self.count()
+        soa = np.zeros((N_PTS_ARRAYS, max(n, 1)), dtype=np.float64)
+        nn = ctypes.c_uint(0)
+        code = LIB.mpm_download_soa(self._h, dptr(soa), soa.shape[1], ctypes.byref(nn))
+        if raise_on_error:
+            check(code, "mpm_download_soa")
+        return soa[:, :nn.value]
+
+    def ids(self):
+        n = self.count()
+        ids = np.zeros(max(n, 1), dtype=np.uint32)
+        nn = ctypes.c_uint(0)
+        check(LIB.mpm_download_ids(self._h, uptr(ids), ctypes.byref(nn)), "mpm_download_ids")
+        return ids[:nn.value]
+
+    def sort(self):
+        return check(LIB.mpm_sort(self._h), "mpm_sort")
+
+    def set_sort_interval(self, k):
+        check(LIB.mpm_set_sort_interval(self._h, k), "mpm_set_sort_interval")
+
+    def update_constants(self, prms=None):
+        if prms is not None:
+            self.prms = prms.copy()
+        check(LIB.mpm_update_constants(self._h, ctypes.byref(self.prms)), "mpm_update_constants")
+
+    def set_stream(self, stream_ptr):
+        check(LIB.mpm_set_stream(self._h, ctypes.c_void_p(stream_ptr)), "mpm_set_stream")
+
+    # -- stepping
+    def step(self, nsteps, want_forces=True, raise_on_error=True):
+        hist = np.zeros((nsteps, 3)) if want_forces else None
+        code = LIB.mpm_step(self._h, nsteps, dptr(hist) if want_forces else None)
+        if raise_on_error:
+            check(code, "mpm_step")
+        return hist if want_forces else code
+
+    def params(self):
+        out = SimParams3D()
+        check(LIB.mpm_get_params(self._h, ctypes.byref(out)), "mpm_get_params")
+        return out
+
+    def sensors(self):
+        p = self.params()
+        s = np.zeros(3 * p.IndenterSubdivisions * p.GridZ)
+        tot = np.zeros(3)
+        check(LIB.mpm_sensors(self._h, dptr(s), dptr(tot)), "mpm_sensors")
+        return s, tot
+
+    def error(self):
+        return LIB.mpm_get_error(self._h)
+
+    def synchronize(self):
+        check(LIB.mpm_synchronize(self._h), "mpm_synchronize")
+
+    # -- phases (GPU_Implementation6 one-partition subset)
+    def reset_grid(self):
+        check(LIB.mpm_reset_grid(self._h), "mpm_reset_grid")
+
+    def p2g(self):
+        check(LIB.mpm_p2g(self._h), "mpm_p2g")
+
+    def update_nodes(self, ind_x, ind_y):
+        check(LIB.mpm_update_nodes(self._h, ind_x, ind_y), "mpm_update_nodes")
+
+    def g2p(self, record_pq):
+        check(LIB.mpm_g2p(self._h, int(bool(record_pq))), "mpm_g2p")
+
+    def reset_indenter_force_accumulator(self):
+        check(LIB.mpm_reset_indenter_force_accumulator(self._h), "mpm_reset_indenter_force_accumulator")
+
+    def grid(self):
+        p = self.prms
+        nodes = (p.GridXTotal + 2 * p.GridHaloSize) * p.GridY * p.GridZ
+        g = np.zeros((4, nodes))
+        check(LIB.mpm_testing_download_grid(self._h, dptr(g)), "mpm_testing_download_grid")
+        return g
+
+    def set_p2g_variant(self, v):
+        check(LIB.mpm_testing_set_p2g_variant(self._h, v), "mpm_testing_set_p2g_variant")
+
+
+class GPU_Implementation6:
+    """Method-for-method mirror of the reference class for one partition."""
+
+    def __init__(self, prms, precision=PRECISION_FP64, device=0):
+        self.prms = prms
+        self.precision = precision
+        self.device = device
+        self.handle = None
+        self.hssoa = None
+        self.indenter_force = np.zeros(3)
+        self.indenter_sensor_total = None
+
+    # initialize + allocate_arrays + update_constants (gpu_implementation6.cpp:380-462, 583)
+    def initialize(self, capacity):
+        self.handle = MPMHandle(self.prms, capacity, self.precision, self.device)
+
+    def allocate_arrays(self):
+        pass
+
+    def split_hssoa_into_partitions(self):
+        pass   # one partition spans the grid
+
+    def transfer_ponts_to_device(self, soa, n=None, cohesion=None):
+        self.hssoa = np.ascontiguousarray(soa, dtype=np.float64)
+        self.handle.upload(self.hssoa, n, cohesion)
+
+    def update_constants(self):
+        self.handle.update_constants(self.prms)
+
+    def reset_grid(self):
+        self.handle.reset_grid()
+
+    def p2g(self):
+        self.handle.p2g()
+
+    def receive_halos(self):
+        pass   # one partition: no halo
+
+    def update_nodes(self):
+        self.handle.update_nodes(self.prms.indenter_x, self.prms.indenter_y)
+
+    def g2p(self, recordPQ, enablePointTransfer=False):
+        self.handle.g2p(recordPQ)
+
+    def receive_points(self):
+        pass   # one partition: no migration
+
+    def record_timings(self, enablePointTransfer=False):
+        pass
+
+    def reset_indenter_force_accumulator(self):
+        self.handle.reset_indenter_force_accumulator()
+
+    def transfer_from_device(self):
+        self.hssoa = self.handle.download()
+        sensor, total = self.handle.sensors()
+        self.indenter_sensor_total = sensor
+        self.indenter_force = total
+        return self.hssoa
+
+    def evaluate_indenter_total_force(self):
+        return self.indenter_force
+
+    def synchronize(self):
+        self.handle.synchronize()
+
+
+class Model3D:
+    """Model3D::Step for one frame of UpdateEveryNthStep substeps, driving the
+    phase API exactly as the reference does (model_3d.cpp:24-112)."""
+
+    def __init__(self, prms, soa, cohesion=None, precision=PRECISION_FP64, device=0):
+        self.prms = prms.copy()
+        self.gpu = GPU_Implementation6(self.prms, precision, device)
+        self.gpu.initialize(soa.shape[1])
+        self.gpu.transfer_ponts_to_device(soa, cohesion=cohesion)
+        self.gpu.update_constants()
+
+    def Step(self, substeps=None):
+        p = self.prms
+        simulation_time = p.SimulationTime
+        count = 0
+        self.gpu.reset_indenter_force_accumulator()
+        n_sub = substeps if substeps is not None else None
+        while True:
+            simulation_time += p.InitialTimeStep
+            p.indenter_x = p.indenter_x_initial + simulation_time * p.IndVelocity
+            self.gpu.reset_grid()
+            self.gpu.p2g()
+            self.gpu.receive_halos()
+            self.gpu.update_nodes()
+            isZeroStep = (p.SimulationStep + count) % p.UpdateEveryNthStep == 0
+            self.gpu.g2p(isZeroStep, False)
+            count += 1
+            if n_sub is not None and count >= n_sub:
+                break
+            if n_sub is None and (p.SimulationStep + count) % p.UpdateEveryNthStep == 0:
+                break
+        p.SimulationTime = simulation_time
+        p.SimulationStep += count
+        self.gpu.transfer_from_device()
+        return p.SimulationTime < p.SimulationEndTime

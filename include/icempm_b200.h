@@ -1,0 +1,179 @@
+/*
+ * icempm_b200 — C-ABI of the B200-native single-partition MLS-MPM step.
+ *
+ * Plain C: an opaque handle, plain pointers and sizes, int status returns.
+ * No exception crosses this boundary. One host thread drives a handle; all
+ * device work of a handle is issued on one CUDA stream (its own, or the one
+ * given to mpm_set_stream).
+ *
+ * Each entry point names the reference interface it replaces
+ * (paths relative to the reference project root).
+ *
+ * Status codes
+ *   0          ok
+ *   70..75     a particle left the grid in -x/-y/-z/+x/+y/+z
+ *              (the device error byte of mpm_kernels.cuh:70-75)
+ *   5          receive overflow (mpm_kernels.cuh:420; never raised with one
+ *              partition, kept for the numbering)
+ *   >= 100     new codes of this library, listed below
+ */
+#ifndef ICEMPM_B200_H
+#define ICEMPM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "sim_params_3d.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPM_OK                 0
+#define MPM_ERR_RECEIVE        5
+#define MPM_ERR_OUT_XMIN      70
+#define MPM_ERR_OUT_YMIN      71
+#define MPM_ERR_OUT_ZMIN      72
+#define MPM_ERR_OUT_XMAX      73
+#define MPM_ERR_OUT_YMAX      74
+#define MPM_ERR_OUT_ZMAX      75
+#define MPM_ERR_CUDA         100  /* a CUDA runtime call failed              */
+#define MPM_ERR_ARG          101  /* invalid argument (null, size, mode)     */
+#define MPM_ERR_CAPACITY     102  /* more particles than the handle holds    */
+#define MPM_ERR_NO_DEVICE    103  /* no CUDA device / wrong architecture     */
+#define MPM_ERR_CONFIG_FILE  104  /* configuration file missing / unreadable */
+#define MPM_ERR_CONFIG_JSON  105  /* not JSON, or a key of the wrong type    */
+#define MPM_ERR_CONFIG_KEY   106  /* required key "InputRawPoints" missing   */
+#define MPM_ERR_SORT_RANGE   107  /* a particle's cell key lies outside grid */
+#define MPM_ERR_STATE        108  /* call out of order (e.g. step before upload) */
+
+#define MPM_PRECISION_FP64   0    /* FP64 state and transfers; 3x3 SVD in FP32
+                                     exactly as the reference (helper_math.cuh) */
+#define MPM_PRECISION_MIXED  1    /* FP32 state and transfers, fixed-point grid
+                                     accumulation; FP64 SVD, apex return map and
+                                     indenter force reduction                 */
+#define MPM_PRECISION_FP64_SVD64 2 /* FP64 throughout, SVD included: the
+                                     high-accuracy reference of the mixed mode */
+
+typedef struct mpm_handle mpm_handle;
+
+/* ---------------------------------------------------------------- params */
+
+/* SimParams3D::Reset (parameters_sim_3d.cpp:5-62). */
+void mpm_params_reset(SimParams3D* prms);
+/* SimParams3D::ComputeLame (parameters_sim_3d.cpp:164-169). */
+void mpm_params_compute_lame(SimParams3D* prms);
+/* SimParams3D::ComputeCamClayParams (parameters_sim_3d.cpp:171-175). */
+void mpm_params_compute_camclay(SimParams3D* prms);
+/* SimParams3D::ComputeHelperVariables (parameters_sim_3d.cpp:65-86). */
+void mpm_params_compute_helper_variables(SimParams3D* prms);
+/* SimParams3D::SetPhi (parameters_sim_3d.h:100), angle in degrees. */
+void mpm_params_set_phi(SimParams3D* prms, double phi_degrees);
+/* SimParams3D::ParseFile (parameters_sim_3d.cpp:89-162): Reset, then read the
+ * same JSON keys, then derive. The value of "InputRawPoints" is copied into
+ * raw_points_file (NUL-terminated, truncated to buflen). Returns 0, or
+ * MPM_ERR_CONFIG_FILE / _JSON / _KEY where the reference throws. */
+int  mpm_params_parse_file(SimParams3D* prms, const char* path,
+                           char* raw_points_file, int buflen);
+/* Same as mpm_params_parse_file on an in-memory JSON text. */
+int  mpm_params_parse_string(SimParams3D* prms, const char* json_text,
+                             char* raw_points_file, int buflen);
+
+/* ---------------------------------------------------------------- handle */
+
+/* GPU_Implementation6::initialize + allocate_arrays + update_constants
+ * (gpu_implementation6.cpp:380-398, 446-462, 583-586;
+ *  gpu_partition_3d.cu:218-309). One partition on `device`.
+ * `capacity` = number of particles the handle can hold. The grid is
+ * GridXTotal x GridY x GridZ nodes (no halo slabs: one partition).
+ * *status receives 0 or an error code; NULL is returned on error. */
+mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity,
+                       int device, int* status);
+/* ~GPU_Partition_3D (gpu_partition_3d.cu:193-216). */
+void mpm_destroy(mpm_handle* h);
+/* Issue all later work of h on `cuda_stream` (a cudaStream_t); NULL restores
+ * the handle's own stream. */
+int  mpm_set_stream(mpm_handle* h, void* cuda_stream);
+/* GPU_Implementation6::update_constants (gpu_implementation6.cpp:583-586;
+ * gpu_partition_3d.cu:301-309): copies the parameter block to the device and
+ * clears the device error byte. The grid dimensions must not change. */
+int  mpm_update_constants(mpm_handle* h, const SimParams3D* prms);
+
+/* -------------------------------------------------------- particle data */
+
+/* GPU_Implementation6::transfer_ponts_to_device (gpu_implementation6.cpp:465-475;
+ * gpu_partition_3d.cu:367-381): n particles from a host SoA in the
+ * reference's HostSideSOA row layout (row k at soa + k*pitch, 28 rows). */
+int  mpm_upload_soa(mpm_handle* h, const double* soa, unsigned pitch, unsigned n);
+/* New per-particle field (no reference counterpart): cohesion c_i in Pa.
+ * The Drucker-Prager apex shift becomes p0_i = c_i / DP_tan_phi in place of
+ * the global DP_threshold_p (mpm_kernels.cuh:499,505-509,525). NULL clears
+ * the field and restores the global value. */
+int  mpm_upload_cohesion(mpm_handle* h, const double* cohesion, unsigned n);
+/* GPU_Implementation6::transfer_from_device (gpu_implementation6.cpp:478-557;
+ * gpu_partition_3d.cu:335-365): writes the particles in the handle's current
+ * order into the host SoA (28 rows, row stride pitch >= n), *n = count.
+ * Returns the device error code (70..75) if one was raised, as the
+ * reference throws on it. */
+int  mpm_download_soa(mpm_handle* h, double* soa, unsigned pitch, unsigned* n);
+/* New: the upload index of each particle in the current order (the sort of
+ * mpm_sort permutes particles; this gives the permutation). */
+int  mpm_download_ids(mpm_handle* h, unsigned* ids, unsigned* n);
+/* HostSideSOA::RemoveDisabledAndSort (host_side_soa.cpp:56-67) on the device:
+ * drops disabled particles and orders the rest by the cell key of
+ * ProxyPoint3D::getCellIndex (proxypoint3d.cpp:158-163), stable (ties keep
+ * their previous order). */
+int  mpm_sort(mpm_handle* h);
+/* Sort automatically every k substeps inside mpm_step (0 = never, the
+ * default, as with one partition the reference never re-sorts). */
+int  mpm_set_sort_interval(mpm_handle* h, int k);
+
+/* ------------------------------------------ substep phases (one partition) */
+
+/* GPU_Implementation6::reset_grid (gpu_implementation6.cpp:18-29). */
+int  mpm_reset_grid(mpm_handle* h);
+/* GPU_Implementation6::p2g (gpu_implementation6.cpp:31-77). */
+int  mpm_p2g(mpm_handle* h);
+/* GPU_Implementation6::update_nodes (gpu_implementation6.cpp:115-123); the
+ * indenter centre is passed by value as in gpu_partition_3d.cu:416-419. */
+int  mpm_update_nodes(mpm_handle* h, double indenter_x, double indenter_y);
+/* GPU_Implementation6::g2p (gpu_implementation6.cpp:125-133); record_pq as
+ * recordPQ (mpm_kernels.cuh:347-351). */
+int  mpm_g2p(mpm_handle* h, int record_pq);
+/* GPU_Implementation6::reset_indenter_force_accumulator
+ * (gpu_implementation6.cpp:527; gpu_partition_3d.cu:311-316). */
+int  mpm_reset_indenter_force_accumulator(mpm_handle* h);
+
+/* ---------------------------------------------------------------- driver */
+
+/* The substep loop of Model3D::Step (model_3d.cpp:35-51) for nsteps
+ * substeps: SimulationTime += dt; indenter_x = indenter_x_initial +
+ * SimulationTime*IndVelocity; reset grid, P2G, grid update, G2P (P,Q
+ * recorded when SimulationStep % UpdateEveryNthStep == 0);
+ * SimulationStep += 1. force_hist (host, may be NULL) receives nsteps x 3
+ * doubles: the total force on the indenter of each substep (sum over the
+ * sensor bins of that substep, N). Returns the device error code if one was
+ * raised during these substeps. */
+int  mpm_step(mpm_handle* h, int nsteps, double* force_hist);
+/* The frame-level sensor readout of transfer_from_device
+ * (gpu_implementation6.cpp:499-520): sensor receives
+ * 3*IndenterSubdivisions*GridZ doubles, each divided by
+ * UpdateEveryNthStep*cellsize^2; total receives the summed force divided by
+ * UpdateEveryNthStep (evaluate_indenter_total_force, :560-571). */
+int  mpm_sensors(mpm_handle* h, double* sensor, double total[3]);
+/* The device error byte (gpu_error_indicator, mpm_kernels.cuh:17). */
+int  mpm_get_error(mpm_handle* h);
+/* GPU_Implementation6::synchronize (gpu_implementation6.cpp:574-581). */
+int  mpm_synchronize(mpm_handle* h);
+/* Read back the handle's copy of the parameter block (SimulationTime,
+ * SimulationStep, indenter_x advance inside mpm_step). */
+int  mpm_get_params(mpm_handle* h, SimParams3D* out);
+/* Number of particles currently held (after sorts that drop disabled ones). */
+int  mpm_count(mpm_handle* h, unsigned* n);
+/* Text of the last CUDA failure seen by this thread (MPM_ERR_CUDA). */
+const char* mpm_last_error_string(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ICEMPM_B200_H */

@@ -1,0 +1,144 @@
+"""CPU ORACLE — test infrastructure, not product code.
+
+ctypes bindings of oracle/liboracle.so (the C++ restatement of the
+reference step, see mpm_oracle.h) and of oracle/_ref/libref_svd.so (the
+reference's own helper_math.cuh SVD compiled on the host). Only tests/,
+__graft_entry__.smoke() and bench.py's cpu_baseline leg import this module.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_dp = ctypes.POINTER(ctypes.c_double)
+_up = ctypes.POINTER(ctypes.c_uint)
+
+
+def _ptr(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def _load():
+    path = os.path.join(_HERE, "liboracle.so")
+    if not os.path.exists(path):
+        raise RuntimeError("oracle/liboracle.so is not built: run `make -C oracle`")
+    lib = ctypes.CDLL(path)
+    lib.or_grid_nodes.restype = ctypes.c_longlong
+    lib.or_grid_nodes.argtypes = [ctypes.c_void_p]
+    lib.or_svd3x3_f32.argtypes = [_dp, _dp, _dp, _dp]
+    lib.or_svd3x3_f64.argtypes = [_dp, _dp, _dp, _dp, ctypes.c_int]
+    lib.or_cell_key.restype = ctypes.c_int
+    lib.or_cell_key.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    lib.or_sort_permutation.restype = ctypes.c_uint
+    lib.or_sort_permutation.argtypes = [ctypes.c_void_p, _dp, ctypes.c_uint, ctypes.c_uint, _up]
+    lib.or_p2g.restype = ctypes.c_int
+    lib.or_p2g.argtypes = [ctypes.c_void_p, _dp, ctypes.c_uint, ctypes.c_uint, _dp, ctypes.c_int]
+    lib.or_update_nodes.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp, ctypes.c_int]
+    lib.or_g2p.restype = ctypes.c_int
+    lib.or_g2p.argtypes = [ctypes.c_void_p, _dp, ctypes.c_uint, ctypes.c_uint, _dp, ctypes.c_int, _dp,
+                           ctypes.c_int, ctypes.c_int]
+    lib.or_step.restype = ctypes.c_int
+    lib.or_step.argtypes = [ctypes.c_void_p, _dp, ctypes.c_uint, ctypes.c_uint, _dp, _dp, _dp, _dp,
+                            ctypes.c_int, ctypes.c_int]
+    return lib
+
+
+LIB = _load()
+
+
+def ref_svd_lib():
+    """The reference's own SVD compiled on the host, or None if not built."""
+    path = os.path.join(_HERE, "_ref", "libref_svd.so")
+    if not os.path.exists(path):
+        return None
+    lib = ctypes.CDLL(path)
+    lib.ref_svd3x3.argtypes = [_dp, _dp, _dp, _dp]
+    return lib
+
+
+def svd(a, mode="f32", sweeps=8):
+    """3x3 SVD of the oracle: mode f32 = reference semantics, f64 = double."""
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(9)
+    u = np.zeros(9); s = np.zeros(3); v = np.zeros(9)
+    if mode == "f32":
+        LIB.or_svd3x3_f32(_ptr(a), _ptr(u), _ptr(s), _ptr(v))
+    else:
+        LIB.or_svd3x3_f64(_ptr(a), _ptr(u), _ptr(s), _ptr(v), sweeps)
+    return u.reshape(3, 3), s, v.reshape(3, 3)
+
+
+def ref_svd(a):
+    lib = ref_svd_lib()
+    if lib is None:
+        raise RuntimeError("oracle/_ref/libref_svd.so is not built")
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(9)
+    u = np.zeros(9); s = np.zeros(3); v = np.zeros(9)
+    lib.ref_svd3x3(_ptr(a), _ptr(u), _ptr(s), _ptr(v))
+    return u.reshape(3, 3), s, v.reshape(3, 3)
+
+
+def grid_nodes(prms):
+    return int(LIB.or_grid_nodes(ctypes.byref(prms)))
+
+
+def cell_key(prms, x, y, z):
+    return LIB.or_cell_key(ctypes.byref(prms), x, y, z)
+
+
+def sort_permutation(prms, soa, n):
+    """Stable RemoveDisabledAndSort permutation over the first n particles."""
+    soa = np.ascontiguousarray(soa, dtype=np.float64)
+    pitch = soa.shape[1]
+    perm = np.zeros(n, dtype=np.uint32)
+    m = LIB.or_sort_permutation(ctypes.byref(prms), _ptr(soa), pitch, n, _ptr(perm, _up))
+    return perm[:m]
+
+
+def p2g(prms, soa, n, nthreads=1):
+    grid = np.zeros((4, grid_nodes(prms)))
+    pitch = soa.shape[1]
+    err = LIB.or_p2g(ctypes.byref(prms), _ptr(soa), pitch, n, _ptr(grid), nthreads)
+    return grid, err
+
+
+def update_nodes(prms, grid, ind_x, ind_y, sensor=None, nthreads=1):
+    f = np.zeros(3)
+    if sensor is None:
+        sensor = np.zeros(3 * prms.IndenterSubdivisions * prms.GridZ)
+    LIB.or_update_nodes(ctypes.byref(prms), _ptr(grid), ind_x, ind_y, _ptr(sensor), _ptr(f), nthreads)
+    return f, sensor
+
+
+def g2p(prms, soa, n, grid, record_pq=False, p0=None, svd_mode=0, nthreads=1):
+    p0p = _ptr(p0) if p0 is not None else None
+    return LIB.or_g2p(ctypes.byref(prms), _ptr(soa), soa.shape[1], n, _ptr(grid), int(record_pq), p0p,
+                      svd_mode, nthreads)
+
+
+class OracleSim:
+    """Runs substeps of Model3D::Step on a private copy of the SoA."""
+
+    def __init__(self, prms, soa, n, p0=None, svd_mode=0, nthreads=1):
+        import copy
+        self.prms = copy.copy(prms)
+        self.soa = np.array(soa, dtype=np.float64, copy=True, order="C")
+        self.n = n
+        self.p0 = None if p0 is None else np.ascontiguousarray(p0, dtype=np.float64)
+        self.svd_mode = svd_mode
+        self.nthreads = nthreads
+        self.grid = np.zeros((4, grid_nodes(self.prms)))
+        self.sensor = np.zeros(3 * self.prms.IndenterSubdivisions * self.prms.GridZ)
+
+    def step(self, nsteps=1):
+        hist = np.zeros((nsteps, 3))
+        err = 0
+        f = np.zeros(3)
+        p0p = _ptr(self.p0) if self.p0 is not None else None
+        for s in range(nsteps):
+            e = LIB.or_step(ctypes.byref(self.prms), _ptr(self.soa), self.soa.shape[1], self.n, _ptr(self.grid),
+                            _ptr(self.sensor), _ptr(f), p0p, self.svd_mode, self.nthreads)
+            hist[s] = f
+            if e and not err:
+                err = e
+        return hist, err
