@@ -1,0 +1,347 @@
+"""Benchmark of the single-partition MLS-MPM step (particle-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload block8m] [--precision mixed|fp64]
+
+Workload: the 8,000,000-particle block of the mixed-precision target
+configuration (4.0 x 1.0 x 1.0 m, h = 0.01 m, dt = 5e-6 s, lognormal cohesion
+median 3e5 Pa sigma_log 0.3, indenter 1.0 m/s), seeded synthetic jittered
+lattice. One "step" is one substep of Model3D::Step on the whole block.
+
+value: particle-steps/s over all ranks with the state resident on the device
+(timed with CUDA events on the handle's stream, barrier + synchronize on both
+sides, max over ranks). e2e: the same metric through the public C-ABI with
+host buffers (pinned SoA uploaded, K substeps with the force history read
+back, SoA downloaded) inside the timed region. N > 1 runs independent
+replicas, one per GPU (the path is one partition; no collective).
+
+--impl reference times the CPU port of the reference step (the oracle,
+OpenMP on all host cores) on the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+B_PARTICLE = {"mixed": 208, "fp64": 416}       # bytes per particle-step (state read + write)
+B_COHESION = {"mixed": 4, "fp64": 8}           # per-particle cohesion read
+B_NODE = {"mixed": 32, "fp64": 64}             # bytes per active node per step
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="block8m")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def init_dist(world, backend):
+    if world <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def max_over_ranks(dist, value, device):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_per_particle(kernel, precision):
+    """DRAM bytes per particle of the dominant kernel from the committed ncu
+    summary (profiles/), captured on a smaller block and scaled by particles."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{precision}.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_particle:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(cfg_name, seconds, threads=None):
+    """The CPU port of the reference step (oracle, FP64, OpenMP over all host
+    cores) on the same block: warm-up 1 substep, then substeps until
+    `seconds` have elapsed (at least 2)."""
+    from icempm_3dm_b200 import generator as gen
+    from oracle import pyoracle as po
+    threads = threads or os.cpu_count() or 1
+    prms, soa, coh = gen.make_block(gen.CONFIGS[cfg_name])
+    n = soa.shape[1]
+    p0 = None if coh is None else coh / prms.DP_tan_phi
+    sim = po.OracleSim(prms, soa, n, p0=p0, svd_mode=0, nthreads=threads)
+    sim.step(1)
+    t0 = time.perf_counter()
+    done = 0
+    while done < 2 or time.perf_counter() - t0 < seconds:
+        sim.step(1)
+        done += 1
+    dt = time.perf_counter() - t0
+    return {"value": n * done / dt, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{done} substeps of the full {n}-particle block after 1 warm-up substep "
+                      f"(oracle/liboracle.so, FP64, OpenMP {threads} threads)"}
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from icempm_3dm_b200 import generator as gen
+    from oracle import pyoracle as po
+    threads = os.cpu_count() or 1
+    cfg = gen.CONFIGS[args.workload]
+    prms, soa, coh = gen.make_block(cfg)
+    n = soa.shape[1]
+    p0 = None if coh is None else coh / prms.DP_tan_phi
+    sim = po.OracleSim(prms, soa, n, p0=p0, svd_mode=0, nthreads=threads)
+    sim.step(max(1, min(args.warmup, 3)))
+    t0 = time.perf_counter()
+    sim.step(args.steps)
+    dt = time.perf_counter() - t0
+    value = n * args.steps / dt
+    out = {"impl": "reference", "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+           "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "config": {"workload": args.workload, "particles": n},
+           "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+                            "sample": f"{args.steps} substeps of the full block (oracle port of the reference "
+                                      f"step, FP64, OpenMP)"},
+           "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_env()
+    if world != args.gpus and world > 1:
+        print(f"warning: WORLD_SIZE {world} != --gpus {args.gpus}", file=sys.stderr)
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist = init_dist(world, "nccl")
+
+    from icempm_3dm_b200 import MPMHandle, PRECISION_FP64, PRECISION_MIXED
+    from icempm_3dm_b200 import generator as gen
+    prec = PRECISION_MIXED if args.precision == "mixed" else PRECISION_FP64
+    cfg = gen.CONFIGS[args.workload]
+    prms, soa, coh = gen.make_block(cfg)
+    n = soa.shape[1]
+    stream = torch.cuda.Stream(device=device)
+
+    h = MPMHandle(prms, n, prec, device=local)
+    h.set_stream(stream.cuda_stream)
+    h.upload(soa, cohesion=coh)
+    h.sort()
+    h.step(max(args.warmup, 3), want_forces=False)
+
+    # --- device-resident throughput
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    hist = h.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(device)
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(dist, ms, device)
+    value = world * n * args.steps / (ms_max * 1e-3)
+
+    # --- per-kernel timing (CUDA events on the handle's stream, in-library)
+    kms = h.step_timed(args.steps)
+    active = h.active_nodes()
+    if prec == PRECISION_MIXED:
+        dom_name, dom_ms = "k_g2p2g_mixed", kms[3] / args.steps
+        dom_bytes = n * (B_PARTICLE["mixed"] + (B_COHESION["mixed"] if coh is not None else 0)) + \
+            active * B_NODE["mixed"]
+        launches_per_step = 2
+    else:
+        names = ["grid clear", "k_p2g", "k_update_f64", "k_g2p_f64"]
+        k = int(np.argmax(kms[1:])) + 1
+        dom_name, dom_ms = names[k], kms[k] / args.steps
+        # FP64 form: P2G reads 200 B (x, v, F, C), G2P reads 112 B and writes 208 B
+        per = {1: 200, 3: 320}.get(k, 0)
+        dom_bytes = n * per + (active * 32 if k in (1, 3) else active * 64)
+        launches_per_step = 3
+    peak, peak_kind = measured_peak_hbm()
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    tpp = traffic_per_particle(dom_name, args.precision)
+    step_bytes = n * (B_PARTICLE[args.precision] + (B_COHESION[args.precision] if coh is not None else 0)) + \
+        active * B_NODE[args.precision]
+
+    # --- end to end through the C-ABI with pinned host buffers
+    host = torch.empty(soa.shape, dtype=torch.float64, pin_memory=True)
+    host.numpy()[...] = soa
+    host_np = host.numpy()
+    out_host = torch.empty(soa.shape, dtype=torch.float64, pin_memory=True).numpy()
+    h2 = MPMHandle(prms, n, prec, device=local)
+    h2.set_stream(stream.cuda_stream)
+    h2.upload(host_np, cohesion=coh)
+    h2.step(3, want_forces=False)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    h2.upload(host_np, cohesion=coh)
+    h2.step(args.steps)
+    from icempm_3dm_b200._lib import LIB, dptr
+    import ctypes
+    nn = ctypes.c_uint(0)
+    LIB.mpm_download_soa(h2._h, dptr(out_host), out_host.shape[1], ctypes.byref(nn))
+    f1.record(stream)
+    f1.synchronize()
+    e2e_ms = max_over_ranks(dist, f0.elapsed_time(f1), device)
+    h2.close()
+    soa_bytes = soa.nbytes + (coh.nbytes if coh is not None else 0)
+    e2e = {"value": world * n * args.steps / (e2e_ms * 1e-3), "unit": "particle-steps/s",
+           "h2d_bytes_per_step": soa_bytes / args.steps,
+           "d2h_bytes_per_step": (soa.nbytes + 24 * args.steps) / args.steps}
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(args.workload, args.cpu_seconds)
+
+    if rank == 0:
+        out = {
+            "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if prec == PRECISION_MIXED else "f64",
+            "data": "synthetic: seeded jittered-lattice ice block (shapes of the target configuration)",
+            "config": {"workload": args.workload, "particles": n, "precision": args.precision,
+                       "grid": [prms.GridXTotal, prms.GridY, prms.GridZ], "h": prms.cellsize,
+                       "dt": prms.InitialTimeStep, "parallelism": f"replicas x{world}",
+                       "l2": "state larger than L2 (no flush needed)",
+                       "active_nodes": active, "step_bytes_algorithmic": step_bytes,
+                       "hbm_fraction_step": step_bytes / (ms_max / args.steps * 1e-3) / 1e9 / peak},
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": (tpp * n if tpp else None)},
+            "kernel_ms_per_step": {"update": kms[2] / args.steps,
+                                   ("g2p2g" if prec == PRECISION_MIXED else "g2p"): kms[3] / args.steps,
+                                   **({} if prec == PRECISION_MIXED else {"p2g": kms[1] / args.steps,
+                                                                          "clear": kms[0] / args.steps})},
+            "force_last": hist[-1].tolist(),
+            "cpu_baseline": base, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": launches_per_step * args.steps,
+        }
+        print(json.dumps(out), flush=True)
+    h.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -304,6 +304,123 @@ __global__ void __launch_bounds__(BLOCK) k_p2g_tile_f64(DevParams P, const doubl
     }
 }
 
+// Variant 4 (default): block fixed-point tile.
+//
+// A block takes a chunk of BLOCK*PPT consecutive particles of the sorted
+// order. Their 27-node stencils fall in a small box of nodes, accumulated in
+// shared memory as 64-bit integers: value v is stored as round(v * 2^e),
+// with e chosen so that the box can absorb the chunk's contributions without
+// overflow (a per-chunk bound on |contribution| measured in the previous
+// launch, with margin). Integer sums are exact and order-independent, so the
+// tile result does not depend on thread scheduling; the resolution 2^-e is
+// ~2^-50 of the chunk's largest contribution, the rounding level of an FP64
+// sum. Contributions beyond the bound (a particle that sped up, the first
+// launch) go straight to the grid with FP64 atomics. The tile is converted
+// back to FP64 and added to the grid once per node.
+constexpr int kFxHeadroomBits = 10;          // up to 1024 contributions per node
+constexpr double kFxMaxUnits = 4503599627370496.0;   // 2^52: |round(v 2^e)| limit
+
+__device__ __forceinline__ int fx_exponent(double bound) {
+    // smallest e with bound * 2^e <= 2^52 (bound includes a 4x margin)
+    int ex;
+    frexp(bound * 4.0, &ex);
+    return 52 - ex;
+}
+
+template <int BLOCK, int PPT>
+__global__ void __launch_bounds__(BLOCK, 2) k_p2g_fx_f64(DevParams P, const double* __restrict__ pts, size_t pitch,
+                                                         int n, double* __restrict__ grid, int* err, int tile_cap,
+                                                         float* __restrict__ chunk_bound) {
+    extern __shared__ long long tl[];
+    __shared__ float s_max;
+    const int chunk0 = blockIdx.x * BLOCK * PPT;
+    // pass A: node box of the chunk's stencils (positions only)
+    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+    for (int k = 0; k < PPT; k++) {
+        const int i = chunk0 + k * BLOCK + threadIdx.x;
+        if (i >= n) break;
+        const long long util = __double_as_longlong(pts[i]);
+        if (util & kDisabled) continue;
+        int b[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) b[d] = (int)(pts[(MPM_POSX + d) * pitch + i] * P.h_inv - 0.5);
+        if (stencil_error(P, b[0], b[1], b[2])) continue;
+#pragma unroll
+        for (int d = 0; d < 3; d++) { lo[d] = min(lo[d], b[d]); hi[d] = max(hi[d], b[d] + 2); }
+    }
+    int blo[3], bhi[3];
+    block_box(lo, hi, blo, bhi);
+    const bool have_box = blo[0] <= bhi[0];
+    const int ex = have_box ? bhi[0] - blo[0] + 1 : 0, ey = have_box ? bhi[1] - blo[1] + 1 : 0,
+              ez = have_box ? bhi[2] - blo[2] + 1 : 0;
+    const long long vol = (long long)ex * ey * ez;
+    const bool use_tile = have_box && vol <= tile_cap;
+    const int nv = use_tile ? (int)vol : 0;
+    if (threadIdx.x == 0) s_max = 0.f;
+    for (int k = threadIdx.x; k < 4 * nv; k += BLOCK) {
+        const int comp = k / nv;
+        tl[comp * tile_cap + (k - comp * nv)] = 0;
+    }
+    __syncthreads();
+
+    const double mmax = fmax(P.particle_mass, P.liquid_mass);
+    const int e_m = fx_exponent(mmax);
+    const float prev = chunk_bound[blockIdx.x];
+    const int e_p = fx_exponent(prev > 0.f ? (double)prev : mmax * 16.0);
+    const double s_m = ldexp(1.0, e_m), s_p = ldexp(1.0, e_p);
+    float my_max = 0.f;
+
+    // pass B: contributions
+    for (int k = 0; k < PPT; k++) {
+        const int i = chunk0 + k * BLOCK + threadIdx.x;
+        if (i >= n) break;
+        P2GPoint q;
+        if (!p2g_prepare(P, pts, pitch, i, q, err)) continue;
+        const bool in_tile = use_tile && !stencil_error(P, q.base[0], q.base[1], q.base[2]);
+        if (!in_tile) {
+            p2g_scatter(P, q, [&](int a, int b, int c, double incM, const double incV[3]) {
+                const int x = q.base[0] + a, y = q.base[1] + b, z = q.base[2] + c;
+                if (!node_inside(P, x, y, z)) return;
+                grid_atomic_add(grid, P.gstride, node_index(P, x, y, z), incM, incV);
+            });
+            continue;
+        }
+        const int ox = q.base[0] - blo[0], oy = q.base[1] - blo[1], oz = q.base[2] - blo[2];
+        p2g_scatter(P, q, [&](int a, int b, int c, double incM, const double incV[3]) {
+            const int t = ((ox + a) * ey + (oy + b)) * ez + (oz + c);
+            const double am = fmax(fabs(incV[0]), fmax(fabs(incV[1]), fabs(incV[2])));
+            my_max = fmaxf(my_max, (float)am);
+            if (am * s_p < kFxMaxUnits) {
+                atomicAdd((unsigned long long*)(tl + tile_cap + t), (unsigned long long)__double2ll_rn(incV[0] * s_p));
+                atomicAdd((unsigned long long*)(tl + 2 * tile_cap + t), (unsigned long long)__double2ll_rn(incV[1] * s_p));
+                atomicAdd((unsigned long long*)(tl + 3 * tile_cap + t), (unsigned long long)__double2ll_rn(incV[2] * s_p));
+            } else {
+                const long long ni = node_index(P, q.base[0] + a, q.base[1] + b, q.base[2] + c);
+                atomicAdd(grid + P.gstride + ni, incV[0]);
+                atomicAdd(grid + 2 * P.gstride + ni, incV[1]);
+                atomicAdd(grid + 3 * P.gstride + ni, incV[2]);
+            }
+            atomicAdd((unsigned long long*)(tl + t), (unsigned long long)__double2ll_rn(incM * s_m));
+        });
+    }
+    // new bound of this chunk for the next launch
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) my_max = fmaxf(my_max, __shfl_xor_sync(0xffffffffu, my_max, o));
+    if ((threadIdx.x & 31) == 0 && my_max > 0.f) atomicMax((int*)&s_max, __float_as_int(my_max));
+    __syncthreads();
+    if (threadIdx.x == 0) chunk_bound[blockIdx.x] = s_max;
+    // flush: consecutive threads take consecutive tile nodes of one array
+    const double inv_m = ldexp(1.0, -e_m), inv_p = ldexp(1.0, -e_p);
+    for (int k = threadIdx.x; k < 4 * nv; k += BLOCK) {
+        const int comp = k / nv, t = k - comp * nv;
+        const long long u = tl[comp * tile_cap + t];
+        if (u == 0) continue;
+        const double v = (double)u * (comp == 0 ? inv_m : inv_p);
+        const int tz = t % ez, ty = (t / ez) % ey, tx = t / (ez * ey);
+        atomicAdd(grid + comp * P.gstride + node_index(P, blo[0] + tx, blo[1] + ty, blo[2] + tz), v);
+    }
+}
+
 // ----------------------------------------------------------- grid update
 
 // partition_kernel_update_nodes (mpm_kernels.cuh:138-232) for one partition:
@@ -423,17 +540,22 @@ __device__ __forceinline__ void g2p_gather(const DevParams& P, const double* __r
         for (int k = 0; k < 3; k++) C[d][k] = 0;
     }
     const double s4 = 4. * P.h_inv;
-#pragma unroll
+    const long long i0 = node_index(P, base[0], base[1], base[2]);
+    const double* gx = grid + P.gstride;
+    const double* gy = grid + 2 * P.gstride;
+    const double* gz = grid + 3 * P.gstride;
+#pragma unroll 1
     for (int a = 0; a < 3; a++)
 #pragma unroll
-        for (int b = 0; b < 3; b++)
+        for (int b = 0; b < 3; b++) {
+            const long long ib = i0 + a * P.slab + b * P.Gz;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const int x = base[0] + a, y = base[1] + b, z = base[2] + c;
                 if (e && !node_inside(P, x, y, z)) continue;
-                const long long ni = node_index(P, x, y, z);
+                const long long ni = ib + c;
                 const double w = ww[a][0] * ww[b][1] * ww[c][2];
-                const double nv[3] = {grid[P.gstride + ni], grid[2 * P.gstride + ni], grid[3 * P.gstride + ni]};
+                const double nv[3] = {__ldg(gx + ni), __ldg(gy + ni), __ldg(gz + ni)};
                 const double dp[3] = {a - fx[0], b - fx[1], c - fx[2]};
                 const double sw = s4 * w;
 #pragma unroll
@@ -443,6 +565,7 @@ __device__ __forceinline__ void g2p_gather(const DevParams& P, const double* __r
                     for (int k = 0; k < 3; k++) C[r][k] += sw * (nv[r] * dp[k]);
                 }
             }
+        }
 }
 
 // The particle update after the gather (mpm_kernels.cuh:307-327).
@@ -482,8 +605,8 @@ __device__ __forceinline__ void g2p_advance(const DevParams& P, double pos[3], c
 }
 
 // partition_kernel_g2p without migration (mpm_kernels.cuh:237-351).
-template <class K>
-__global__ void __launch_bounds__(128) k_g2p_f64(DevParams P, double* __restrict__ pts, size_t pitch, int n,
+template <class K, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_g2p_f64(DevParams P, double* __restrict__ pts, size_t pitch, int n,
                                                  const double* __restrict__ grid, int record_pq,
                                                  const double* __restrict__ p0_arr, int* err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -1,0 +1,530 @@
+// Mixed-precision step: FP32 particle state and transfers, FP64 where the
+// north-star requires it (3x3 SVD and return map of crushed particles,
+// indenter force reduction).
+//
+// Particle state (SoA, 26 words = 104 B per particle):
+//   int32   X[3]   position in fixed point, x / h * 2^kFixBits
+//   float   v[3]   velocity
+//   float   E[9]   F - I (deviation of the elastic deformation gradient from
+//                  the identity, so that J - 1 and dev(F F^T) keep their
+//                  relative precision near the undeformed state)
+//   float   C[9]   APIC affine matrix ("Bp")
+//   float   Jp_inv
+//   int32   status (low 32 bits of the reference's utility word)
+// optional float p0 (apex shift from cohesion), and float P, Q rows written
+// on record steps.
+//
+// Grid: acc = float4 {m, m vx, m vy, m vz} per node, accumulated with
+// warp-aggregated vector atomics; vel = float4 {vx, vy, vz, 0} per node,
+// written by the node update (which also clears acc for the next P2G).
+// One step is two kernels: node update, then the fused G2P->P2G kernel
+// (G2P of this step and P2G of the next read each particle once).
+#pragma once
+
+#include "device_common.cuh"
+#include "physics_f64.cuh"
+
+namespace icempm {
+
+constexpr int kFixBits = 20;
+constexpr float kFixScale = 1048576.0f;           // 2^20
+constexpr float kFixInv = 9.5367431640625e-07f;   // 2^-20
+
+struct MixedState {
+    int* X;          // 3 rows
+    float* v;        // 3 rows
+    float* E;        // 9 rows
+    float* C;        // 9 rows
+    float* Jp;       // 1 row
+    int* status;     // 1 row
+    float* p0;       // 1 row or null
+    float* PQ;       // 2 rows (P, Q)
+    size_t pitch;
+};
+
+// base = (int)(x/h - 0.5) with C truncation, fx = x/h - base, from the
+// fixed-point coordinate (exact: fx has 21 significant bits)
+__device__ __forceinline__ void fix_base(int X, int& base, float& fx) {
+    const int num = X - (1 << (kFixBits - 1));
+    base = num / (1 << kFixBits);
+    fx = (float)(X - base * (1 << kFixBits)) * kFixInv;
+}
+
+// J - 1 = det(I + E) - 1 without cancellation
+__device__ __forceinline__ float detm1(const float E[3][3]) {
+    const float tr = E[0][0] + E[1][1] + E[2][2];
+    const float m2 = (E[0][0] * E[1][1] - E[0][1] * E[1][0]) + (E[0][0] * E[2][2] - E[0][2] * E[2][0]) +
+                     (E[1][1] * E[2][2] - E[1][2] * E[2][1]);
+    const float d = E[0][0] * (E[1][1] * E[2][2] - E[2][1] * E[1][2]) -
+                    E[1][0] * (E[0][1] * E[2][2] - E[2][1] * E[0][2]) +
+                    E[2][0] * (E[0][1] * E[1][2] - E[1][1] * E[0][2]);
+    return tr + m2 + d;
+}
+
+// dev(F F^T) with F = I + E: dev(E + E^T + E E^T)
+__device__ __forceinline__ void dev_b(const float E[3][3], float D[3][3]) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            D[i][j] = E[i][j] + E[j][i] + (E[i][0] * E[j][0] + E[i][1] * E[j][1] + E[i][2] * E[j][2]);
+    const float t = (D[0][0] + D[1][1] + D[2][2]) * (1.0f / 3.0f);
+    D[0][0] -= t; D[1][1] -= t; D[2][2] -= t;
+}
+
+// Kirchhoff stress (mpm_kernels.cuh:547-557) from E
+__device__ __forceinline__ void kirchhoff_mixed(const DevParams& P, const float E[3][3], float tau[3][3]) {
+    const float jm1 = detm1(E);
+    const float J = 1.0f + jm1;
+    float D[3][3];
+    dev_b(E, D);
+    const float s = (float)P.mu * exp2f(-(2.0f / 3.0f) * log2f(J));
+    const float hyd = (float)(P.kappa * 0.5) * (jm1 * (J + 1.0f));
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) tau[i][j] = s * D[i][j] + (i == j ? hyd : 0.0f);
+}
+
+// Trial p, q (mpm_kernels.cuh:477-484) from E
+__device__ __forceinline__ void trial_pq_mixed(const DevParams& P, const float E[3][3], float& jm1, float& p_tr,
+                                               float& q_tr) {
+    jm1 = detm1(E);
+    const float J = 1.0f + jm1;
+    p_tr = -(float)(0.5 * P.kappa) * (jm1 * (J + 1.0f));
+    float D[3][3];
+    dev_b(E, D);
+    float sq = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) sq += D[i][j] * D[i][j];
+    q_tr = (float)(kCoeff1 * P.mu) * exp2f(-(2.0f / 3.0f) * log2f(J)) * sqrtf(sq);
+}
+
+// ------------------------------------------------------------- G2P part
+
+// Gathers v and C from the float4 velocity grid (mpm_kernels.cuh:278-305).
+// Node indices step from the base node by constant offsets (32-bit: the
+// handle checks that the grid has fewer than 2^31 nodes).
+__device__ __forceinline__ void g2p_gather_mixed(const DevParams& P, const float4* __restrict__ vel, const int base[3],
+                                                 const float fx[3], float v[3], float C[3][3], bool check) {
+    float ww[3][3];
+    quad_weights<float>(fx, ww);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        v[d] = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; k++) C[d][k] = 0.f;
+    }
+    const float s4 = 4.0f * (float)P.h_inv;
+    const int slab = (int)P.slab, gz = P.Gz;
+    const int i0 = ((base[0] + P.halo) * P.Gy + base[1]) * gz + base[2];
+#pragma unroll 1
+    for (int a = 0; a < 3; a++) {
+        const float wa = ww[a][0];
+        const float dpa = a - fx[0];
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            const float wab = wa * ww[b][1];
+            const float dpb = b - fx[1];
+            const int ib = i0 + a * slab + b * gz;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                if (check && !node_inside(P, base[0] + a, base[1] + b, base[2] + c)) continue;
+                const float4 nd = __ldg(vel + ib + c);
+                const float w = wab * ww[c][2];
+                const float nv[3] = {nd.x, nd.y, nd.z};
+                const float dp[3] = {dpa, dpb, c - fx[2]};
+                const float sw = s4 * w;
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    v[r] += w * nv[r];
+                    const float swv = sw * nv[r];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) C[r][k] += swv * dp[k];
+                }
+            }
+        }
+    }
+}
+
+// Return map of a crushed point in FP64 (mpm_kernels.cuh:486-544), E in/out.
+__device__ __noinline__ void return_map_f64(const DevParams& P, float E[3][3], float& Jp, double p0) {
+    double F[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) F[i][j] = (i == j ? 1.0 : 0.0) + (double)E[i][j];
+    double Je, p_tr, q_tr;
+    trial_pq(P, F, Je, p_tr, q_tr);
+    double jp = Jp;
+    drucker_prager_return<SvdF64>(P, F, jp, Je, p_tr, q_tr, p0);
+    Jp = (float)jp;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) E[i][j] = (float)(F[i][j] - (i == j ? 1.0 : 0.0));
+}
+
+// ------------------------------------------------------------- P2G part
+
+// Scatter of one particle (base, fx, m, mv, S) with the warp reduction over
+// lanes sharing a base cell; leaders add float4 {m, mv} to acc.
+__device__ __forceinline__ void p2g_scatter_mixed(const DevParams& P, float4* __restrict__ acc, bool active, bool inside,
+                                                  const int base[3], const float fx[3], float mass, const float mv[3],
+                                                  const float S[3][3], int lane) {
+    const int i0 = ((base[0] + P.halo) * P.Gy + base[1]) * P.Gz + base[2];
+    const int key = inside ? i0 : -1 - lane;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(peers) - 1;
+    const int rounds = (int)__reduce_max_sync(0xffffffffu, (unsigned)(__popc(peers) - 1));
+    float ww[3][3];
+    quad_weights<float>(fx, ww);
+    const float h = (float)P.h;
+    const int slab = (int)P.slab, gz = P.Gz;
+#pragma unroll 1
+    for (int a = 0; a < 3; a++) {
+        const float dx = (a - fx[0]) * h;
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            const float dy = (b - fx[1]) * h;
+            const float wab = ww[a][0] * ww[b][1];
+            const int ib = i0 + a * slab + b * gz;
+            float part[3];
+#pragma unroll
+            for (int m = 0; m < 3; m++) part[m] = mv[m] + S[m][0] * dx + S[m][1] * dy;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float dz = (c - fx[2]) * h;
+                const float W = wab * ww[c][2];
+                float val[4] = {W * mass, W * (part[0] + S[0][2] * dz), W * (part[1] + S[1][2] * dz),
+                                W * (part[2] + S[2][2] * dz)};
+                unsigned rest = peers & ~(1u << leader);
+                for (int k = 0; k < rounds; k++) {
+                    const int src = rest ? __ffs(rest) - 1 : lane;
+                    rest &= rest - 1;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float o = __shfl_sync(0xffffffffu, val[q], src);
+                        if (lane == leader && src != lane) val[q] += o;
+                    }
+                }
+                if (!active || lane != leader) continue;
+                if (!inside && !node_inside(P, base[0] + a, base[1] + b, base[2] + c)) continue;
+                atomicAdd(acc + (ib + c), make_float4(val[0], val[1], val[2], val[3]));
+            }
+        }
+    }
+}
+
+// P2G payload of a particle: S = m C - dt V Dp^-1 tau (mpm_kernels.cuh:63)
+__device__ __forceinline__ void p2g_payload_mixed(const DevParams& P, const float E[3][3], const float C[3][3],
+                                                  const float v[3], bool liquid, float Jp, float& mass, float mv[3],
+                                                  float S[3][3]) {
+    mass = (float)(liquid ? P.liquid_mass : P.particle_mass);
+    float tau[3][3];
+    if (liquid) {
+        const float pw = (float)P.kappa * (1.0f - 1.0f / (Jp * Jp * Jp));
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) tau[i][j] = (i == j) ? pw : 0.f;
+    } else {
+        kirchhoff_mixed(P, E, tau);
+    }
+    const float dvd = (float)P.dt_vol_Dpinv;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        mv[i] = v[i] * mass;
+#pragma unroll
+        for (int j = 0; j < 3; j++) S[i][j] = mass * C[i][j] - dvd * tau[i][j];
+    }
+}
+
+__device__ __forceinline__ void load_mixed(const MixedState& s, int i, int X[3], float E[3][3], float& Jp, int& st) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) X[d] = s.X[d * s.pitch + i];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) E[r][c] = s.E[(3 * r + c) * s.pitch + i];
+    Jp = s.Jp[i];
+    st = s.status[i];
+}
+
+// Standalone P2G from the stored state (first step, phase API).
+__global__ void __launch_bounds__(256) k_p2g_mixed(DevParams P, MixedState s, int n, float4* __restrict__ acc,
+                                                   int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    bool active = i < n;
+    int X[3] = {0, 0, 0}, st = (int)kDisabled;
+    float E[3][3], Jp = 1.f;
+    if (active) load_mixed(s, i, X, E, Jp, st);
+    active = active && !(st & (int)kDisabled);
+    int base[3];
+    float fx[3], mass = 0.f, mv[3] = {0, 0, 0}, S[3][3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) fix_base(X[d], base[d], fx[d]);
+    bool inside = false;
+    if (active) {
+        float v[3], C[3][3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) v[d] = s.v[d * s.pitch + i];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) C[r][c] = s.C[(3 * r + c) * s.pitch + i];
+        p2g_payload_mixed(P, E, C, v, (st & (int)kLiquid) != 0, Jp, mass, mv, S);
+        const int e = stencil_error(P, base[0], base[1], base[2]);
+        if (e) raise_error(err, e);
+        inside = e == 0;
+    } else {
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) S[r][c] = 0.f;
+    }
+    p2g_scatter_mixed(P, acc, active, inside, base, fx, mass, mv, S, lane);
+}
+
+// Fused G2P (this step) -> P2G (next step). do_p2g = 0 gives a plain G2P.
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedState s, int n,
+                                                           const float4* __restrict__ vel, float4* __restrict__ acc,
+                                                           int do_p2g, int record_pq, int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    bool active = i < n;
+    int X[3] = {0, 0, 0}, st = (int)kDisabled;
+    float E[3][3], Jp = 1.f;
+    if (active) load_mixed(s, i, X, E, Jp, st);
+    active = active && !(st & (int)kDisabled);
+
+    int base[3];
+    float fx[3], v[3] = {0, 0, 0}, C[3][3];
+    bool inside = false;
+    if (active) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) fix_base(X[d], base[d], fx[d]);
+        const int e = stencil_error(P, base[0], base[1], base[2]);
+        if (e) raise_error(err, e);
+        g2p_gather_mixed(P, vel, base, fx, v, C, e != 0);
+
+        // advection in fixed point, F <- (I + dt C) F as E <- E + dt C (I + E)
+        const float dt = (float)P.dt;
+        const float adv = dt * (float)P.h_inv * kFixScale;
+#pragma unroll
+        for (int d = 0; d < 3; d++) X[d] += __float2int_rn(v[d] * adv);
+        float En[3][3];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                En[r][c] = E[r][c] + dt * (C[r][c] + (C[r][0] * E[0][c] + C[r][1] * E[1][c] + C[r][2] * E[2][c]));
+        float p_tr = 0.f, q_tr = 0.f;
+        if (st & (int)kLiquid) {
+            float A[3][3];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) A[r][c] = dt * C[r][c];
+            Jp *= 1.0f + detm1(A);
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) E[r][c] = En[r][c];
+        } else {
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) E[r][c] = En[r][c];
+            float jm1;
+            trial_pq_mixed(P, E, jm1, p_tr, q_tr);
+            if (!(st & (int)kCrushed) && outside_failure_surface(P, (short)st, (double)p_tr, (double)q_tr))
+                st |= (int)kCrushed;
+            if (st & (int)kCrushed) {
+                const double p0 = s.p0 ? (double)s.p0[i] : P.p0;
+                return_map_f64(P, E, Jp, p0);
+            }
+        }
+        // store state
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            s.X[d * s.pitch + i] = X[d];
+            s.v[d * s.pitch + i] = v[d];
+        }
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                s.E[(3 * r + c) * s.pitch + i] = E[r][c];
+                s.C[(3 * r + c) * s.pitch + i] = C[r][c];
+            }
+        s.Jp[i] = Jp;
+        s.status[i] = st;
+        if (record_pq) {
+            s.PQ[i] = p_tr;
+            s.PQ[s.pitch + i] = q_tr;
+        }
+    }
+    if (!do_p2g) return;   // uniform across the launch
+    float mass = 0.f, mv[3] = {0, 0, 0}, S[3][3];
+    if (active) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) fix_base(X[d], base[d], fx[d]);
+        p2g_payload_mixed(P, E, C, v, (st & (int)kLiquid) != 0, Jp, mass, mv, S);
+        const int e = stencil_error(P, base[0], base[1], base[2]);
+        if (e) raise_error(err, e);
+        inside = e == 0;
+    } else {
+#pragma unroll
+        for (int d = 0; d < 3; d++) { base[d] = 0; fx[d] = 1.0f; }
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) S[r][c] = 0.f;
+    }
+    p2g_scatter_mixed(P, acc, active, inside, base, fx, mass, mv, S, lane);
+}
+
+// Node update for the mixed grid: FP64 arithmetic on the FP32 sums, contact
+// force in FP64 (sensor and per-substep total), velocities written as float4,
+// the accumulator cleared for the next P2G.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_update_mixed(DevParams P, float4* __restrict__ acc, float4* __restrict__ vel,
+                                                        double ind_x, double ind_y, double* __restrict__ sensor,
+                                                        double* __restrict__ force3) {
+    const long long idx = (long long)blockIdx.x * BLOCK + threadIdx.x;
+    double f[3] = {0, 0, 0};
+    if (idx < P.nodes) {
+        const float4 a = acc[idx];
+        const double mass = a.x;
+        if (mass != 0) {
+            acc[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+            double v[3] = {(double)a.y, (double)a.z, (double)a.w};
+            const int idx_z = (int)(idx % P.Gz);
+            const int idx_y = (int)((idx / P.Gz) % P.Gy);
+            const int idx_x = (int)(idx / P.slab);
+            const int gx = idx_x - P.halo, gy = idx_y, gz = idx_z;
+#pragma unroll
+            for (int k = 0; k < 3; k++) v[k] /= mass;
+            v[1] -= P.dt_gravity;
+            const double vsq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+            if (vsq > P.vmax_sq) {
+                const double nv = sqrt(vsq);
+#pragma unroll
+                for (int k = 0; k < 3; k++) v[k] = v[k] / nv * P.vmax;
+            }
+            if (P.setup_type != 2) {
+                double n0 = gx * P.h - ind_x, n1 = gy * P.h - ind_y;
+                const double nsq = n0 * n0 + n1 * n1;
+                if (nsq < P.ind_rsq) {
+                    const double vrel[3] = {v[0] - P.ind_velocity, v[1], v[2]};
+                    if (nsq > 0) { const double nn = sqrt(nsq); n0 /= nn; n1 /= nn; }
+                    const double vn = vrel[0] * n0 + vrel[1] * n1;
+                    if (vn < 0) {
+                        const double vt[3] = {vrel[0] - n0 * vn, vrel[1] - n1 * vn, vrel[2]};
+                        const double prev[3] = {v[0], v[1], v[2]};
+                        v[0] = P.ind_velocity + vt[0];
+                        v[1] = vt[1];
+                        v[2] = vt[2];
+#pragma unroll
+                        for (int k = 0; k < 3; k++) f[k] = (prev[k] - v[k]) * mass / P.dt;
+                        float angle = atan2f((float)n0, (float)n1);
+                        angle = (float)((double)angle + MPM_PI);
+                        angle = (float)((double)angle * (P.subdiv / (2 * MPM_PI)));
+                        const int ia = min(max((int)angle, 0), P.subdiv - 1);
+                        const int iz = min(max(idx_z, 0), P.Gz - 1);
+                        double* s = sensor + 3 * (iz + ia * P.Gz);
+                        atomicAdd(s + 0, f[0]);
+                        atomicAdd(s + 1, f[1]);
+                        atomicAdd(s + 2, f[2]);
+                    }
+                }
+            }
+            if (P.setup_type != 2) {
+                if (gy <= 2) { v[0] = v[1] = v[2] = 0; }
+            } else {
+                if (gy <= 2 && v[1] < 0) v[1] = 0;
+            }
+            if (gy >= P.Gy - 3 && v[1] > 0) v[1] = 0;
+            if (gx <= 2 && v[0] < 0) v[0] = 0;
+            else if (gx >= P.Gx - 3 && v[0] > 0) v[0] = 0;
+            if (gz <= 2 && v[2] < 0) v[2] = 0;
+            else if (gz >= P.Gz - 3 && v[2] > 0) v[2] = 0;
+            if (P.setup_type == 2 && P.drag != 0) {
+#pragma unroll
+                for (int k = 0; k < 3; k++) v[k] *= (1 - P.drag);
+            }
+            vel[idx] = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
+        }
+    }
+    __shared__ double red[3][BLOCK / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool any = (f[0] != 0) | (f[1] != 0) | (f[2] != 0);
+    if (!__syncthreads_or(any)) return;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        double x = f[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) red[k][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double x = 0;
+        for (int w = 0; w < BLOCK / 32; w++) x += red[threadIdx.x][w];
+        atomicAdd(force3 + threadIdx.x, x);
+    }
+}
+
+// ------------------------------------------- conversion from / to FP64 SoA
+
+__global__ void k_mixed_from_f64(const double* __restrict__ src, size_t spitch, int n, MixedState s, double h_inv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        s.X[d * s.pitch + i] = __double2int_rn(src[(MPM_POSX + d) * spitch + i] * h_inv * (double)(1 << kFixBits));
+        s.v[d * s.pitch + i] = (float)src[(MPM_VELX + d) * spitch + i];
+    }
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            s.E[(3 * r + c) * s.pitch + i] = (float)(src[(MPM_FE00 + 3 * r + c) * spitch + i] - (r == c ? 1.0 : 0.0));
+            s.C[(3 * r + c) * s.pitch + i] = (float)src[(MPM_BP00 + 3 * r + c) * spitch + i];
+        }
+    s.Jp[i] = (float)src[MPM_IDX_JP_INV * spitch + i];
+    s.status[i] = (int)__double_as_longlong(src[i]);
+    s.PQ[i] = (float)src[MPM_IDX_P * spitch + i];
+    s.PQ[s.pitch + i] = (float)src[MPM_IDX_Q * spitch + i];
+}
+
+// The upper 32 bits of the utility word are kept from the uploaded copy
+// (the step only changes the low status bits).
+__global__ void k_mixed_to_f64(MixedState s, int n, double* __restrict__ dst, size_t dpitch, double h) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        dst[(MPM_POSX + d) * dpitch + i] = (double)s.X[d * s.pitch + i] * (1.0 / (double)(1 << kFixBits)) * h;
+        dst[(MPM_VELX + d) * dpitch + i] = (double)s.v[d * s.pitch + i];
+    }
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            dst[(MPM_FE00 + 3 * r + c) * dpitch + i] = (double)s.E[(3 * r + c) * s.pitch + i] + (r == c ? 1.0 : 0.0);
+            dst[(MPM_BP00 + 3 * r + c) * dpitch + i] = (double)s.C[(3 * r + c) * s.pitch + i];
+        }
+    dst[MPM_IDX_JP_INV * dpitch + i] = (double)s.Jp[i];
+    const long long hi = __double_as_longlong(dst[i]) & (long long)0xffffffff00000000LL;
+    dst[i] = __longlong_as_double(hi | (long long)(unsigned)s.status[i]);
+    dst[MPM_IDX_P * dpitch + i] = (double)s.PQ[i];
+    dst[MPM_IDX_Q * dpitch + i] = (double)s.PQ[s.pitch + i];
+}
+
+}  // namespace icempm

@@ -18,9 +18,19 @@
 #include "../../include/icempm_b200_testing.h"
 #include "device_common.cuh"
 #include "kernels_f64.cuh"
+#include "kernels_mixed.cuh"
 #include "sort.cuh"
 
 using namespace icempm;
+
+namespace {
+__global__ void k_narrow(const double* __restrict__ src, float* __restrict__ dst, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = (float)src[i];
+}
+constexpr int kFxBlock = 256;   // threads of the fixed-point P2G
+constexpr int kFxPPT = 4;       // particles per thread (1024-particle chunks)
+}  // namespace
 
 struct mpm_handle {
     SimParams3D prms;
@@ -57,8 +67,22 @@ struct mpm_handle {
     int sort_interval = 0;
     int steps_since_sort = 0;
 
-    int p2g_variant = 0;              // 0 tile (default), 1 direct atomics
+    // mixed precision (MPM_PRECISION_MIXED): 28 rows of 4-byte words
+    // (X 0-2, v 3-5, E 6-14, C 15-23, Jp 24, status 25, P 26, Q 27); the FP64
+    // SoA `pts` is then the staging copy for upload, download and sort
+    void* mx = nullptr;
+    float* p0f = nullptr;
+    float4* gacc = nullptr;
+    float4* gvel = nullptr;
+    bool p2g_ready = false;           // gacc holds the P2G of the current state
+    int mixed_variant = 0;            // fused kernel occupancy target (test hook)
+
+    int p2g_variant = 2;              // see mpm_testing_set_p2g_variant
+    int g2p_variant = 2;              // see mpm_testing_set_g2p_variant
     int tile_cap = 2048;              // P2G tile nodes (x 32 B of shared memory)
+    int fx_tile_cap = 3072;           // nodes of the fixed-point tile (x 32 B)
+    float* chunk_bound = nullptr;     // per-chunk |contribution| bound of the fixed-point P2G
+    int chunk_bound_cap = 0;
     cudaError_t last_cuda = cudaSuccess;
 };
 
@@ -133,6 +157,8 @@ void free_all(mpm_handle* h) {
     cudaFree(h->force_steps); cudaFree(h->force_phase); cudaFree(h->err);
     cudaFree(h->pts_alt); cudaFree(h->p0_alt); cudaFree(h->ids_alt);
     cudaFree(h->s_bucket); cudaFree(h->s_count); cudaFree(h->s_start); cudaFree(h->s_perm);
+    cudaFree(h->chunk_bound);
+    cudaFree(h->mx); cudaFree(h->p0f); cudaFree(h->gacc); cudaFree(h->gvel);
     for (int* p : h->scan_levels) cudaFree(p);
     h->scan_levels.clear();
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -140,11 +166,57 @@ void free_all(mpm_handle* h) {
 
 size_t sensor_count(const SimParams3D& p) { return (size_t)3 * p.IndenterSubdivisions * p.GridZ; }
 
+bool is_mixed(const mpm_handle* h) { return h->precision == MPM_PRECISION_MIXED; }
+
+MixedState mixed_state(mpm_handle* h) {
+    MixedState m;
+    int* wi = static_cast<int*>(h->mx);
+    float* wf = static_cast<float*>(h->mx);
+    const size_t p = h->pitch;
+    m.X = wi;
+    m.v = wf + 3 * p;
+    m.E = wf + 6 * p;
+    m.C = wf + 15 * p;
+    m.Jp = wf + 24 * p;
+    m.status = wi + 25 * p;
+    m.PQ = wf + 26 * p;
+    m.p0 = h->p0f;
+    m.pitch = p;
+    return m;
+}
+
+// staging (FP64 SoA) -> mixed state; p0 (FP64) -> p0f
+int mixed_from_staging(mpm_handle* h) {
+    if (!h->n) return MPM_OK;
+    k_mixed_from_f64<<<blocks_for(h->n, 256), 256, 0, h->stream>>>(h->pts, h->pitch, (int)h->n, mixed_state(h),
+                                                                  h->prms.cellsize_inv);
+    CK_LAUNCH(h, "mixed from f64");
+    if (h->p0) {
+        if (!h->p0f) CK(h, cudaMalloc(&h->p0f, sizeof(float) * h->pitch));
+        k_narrow<<<blocks_for(h->n, 256), 256, 0, h->stream>>>(h->p0, h->p0f, (int)h->n);
+        CK_LAUNCH(h, "p0 narrow");
+    }
+    return MPM_OK;
+}
+
+int mixed_to_staging(mpm_handle* h) {
+    if (!h->n) return MPM_OK;
+    k_mixed_to_f64<<<blocks_for(h->n, 256), 256, 0, h->stream>>>(mixed_state(h), (int)h->n, h->pts, h->pitch,
+                                                                h->prms.cellsize);
+    CK_LAUNCH(h, "mixed to f64");
+    return MPM_OK;
+}
+
 // ---------------------------------------------------------------- phases
 
 int launch_p2g(mpm_handle* h) {
     const int n = (int)h->n;
     if (n == 0) return MPM_OK;
+    if (is_mixed(h)) {
+        k_p2g_mixed<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->dp, mixed_state(h), n, h->gacc, h->err);
+        CK_LAUNCH(h, "p2g mixed");
+        return MPM_OK;
+    }
     const size_t smem = sizeof(double) * 4 * h->tile_cap;
     switch (h->p2g_variant) {
         case 1:
@@ -157,6 +229,20 @@ int launch_p2g(mpm_handle* h) {
             k_p2g_tile_f64<256, true><<<blocks_for(n, 256), 256, smem, h->stream>>>(h->dp, h->pts, h->pitch, n,
                                                                                      h->grid, h->err, h->tile_cap);
             break;
+        case 4: {
+            const int chunks = (int)blocks_for(n, kFxBlock * kFxPPT);
+            if (chunks > h->chunk_bound_cap) {
+                cudaFree(h->chunk_bound);
+    cudaFree(h->mx); cudaFree(h->p0f); cudaFree(h->gacc); cudaFree(h->gvel);
+                h->chunk_bound = nullptr;
+                CK(h, cudaMalloc(&h->chunk_bound, sizeof(float) * chunks));
+                CK(h, cudaMemsetAsync(h->chunk_bound, 0, sizeof(float) * chunks, h->stream));
+                h->chunk_bound_cap = chunks;
+            }
+            k_p2g_fx_f64<kFxBlock, kFxPPT><<<chunks, kFxBlock, sizeof(long long) * 4 * h->fx_tile_cap, h->stream>>>(
+                h->dp, h->pts, h->pitch, n, h->grid, h->err, h->fx_tile_cap, h->chunk_bound);
+            break;
+        }
         default:
             k_p2g_tile_f64<256, false><<<blocks_for(n, 256), 256, smem, h->stream>>>(h->dp, h->pts, h->pitch, n,
                                                                                       h->grid, h->err, h->tile_cap);
@@ -167,27 +253,64 @@ int launch_p2g(mpm_handle* h) {
 }
 
 int launch_update(mpm_handle* h, double ind_x, double ind_y, double* force3) {
+    if (is_mixed(h)) {
+        k_update_mixed<256><<<blocks_for(h->dp.nodes, 256), 256, 0, h->stream>>>(h->dp, h->gacc, h->gvel, ind_x, ind_y,
+                                                                                 h->sensor, force3);
+        CK_LAUNCH(h, "update mixed");
+        return MPM_OK;
+    }
     k_update_f64<256><<<blocks_for(h->dp.nodes, 256), 256, 0, h->stream>>>(h->dp, h->grid, ind_x, ind_y, h->sensor,
                                                                              force3);
     CK_LAUNCH(h, "update kernel");
     return MPM_OK;
 }
 
+int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq) {
+    const int n = (int)h->n;
+    if (n == 0) return MPM_OK;
+    const unsigned nb = blocks_for(n, 128);
+    if (h->mixed_variant == 1)
+        k_g2p2g_mixed<5><<<nb, 128, 0, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g, record_pq,
+                                                    h->err);
+    else if (h->mixed_variant == 2)
+        k_g2p2g_mixed<6><<<nb, 128, 0, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g, record_pq,
+                                                    h->err);
+    else
+        k_g2p2g_mixed<4><<<nb, 128, 0, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g, record_pq,
+                                                    h->err);
+    CK_LAUNCH(h, "g2p2g mixed");
+    return MPM_OK;
+}
+
 int launch_g2p(mpm_handle* h, int record_pq) {
     const int n = (int)h->n;
     if (n == 0) return MPM_OK;
-    if (h->precision == MPM_PRECISION_FP64) {
-        k_g2p_f64<SvdF32><<<blocks_for(n, 128), 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, record_pq,
-                                                                      h->p0, h->err);
-    } else {
-        k_g2p_f64<SvdF64><<<blocks_for(n, 128), 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, record_pq,
-                                                                      h->p0, h->err);
+    if (is_mixed(h)) return launch_g2p2g_mixed(h, 0, record_pq);
+    const unsigned nb = blocks_for(n, 128);
+    const bool f32svd = h->precision == MPM_PRECISION_FP64;
+#define G2P_LAUNCH(MINB)                                                                                        \
+    if (f32svd)                                                                                                 \
+        k_g2p_f64<SvdF32, MINB><<<nb, 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, record_pq, h->p0, \
+                                                           h->err);                                             \
+    else                                                                                                        \
+        k_g2p_f64<SvdF64, MINB><<<nb, 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, record_pq, h->p0, \
+                                                           h->err);
+    switch (h->g2p_variant) {
+        case 1: G2P_LAUNCH(3) break;
+        case 2: G2P_LAUNCH(6) break;
+        default: G2P_LAUNCH(4) break;
     }
+#undef G2P_LAUNCH
     CK_LAUNCH(h, "g2p kernel");
     return MPM_OK;
 }
 
 int reset_grid(mpm_handle* h) {
+    if (is_mixed(h)) {
+        CK(h, cudaMemsetAsync(h->gacc, 0, sizeof(float4) * (size_t)h->dp.nodes, h->stream));
+        h->p2g_ready = false;
+        return MPM_OK;
+    }
     CK(h, cudaMemsetAsync(h->grid, 0, sizeof(double) * 4 * (size_t)h->dp.gstride, h->stream));
     return MPM_OK;
 }
@@ -240,7 +363,18 @@ int exclusive_scan(mpm_handle* h, const int* in, int* out, int n, size_t level) 
     return MPM_OK;
 }
 
+int do_sort_f64(mpm_handle* h);
+
 int do_sort(mpm_handle* h) {
+    if (!is_mixed(h)) return do_sort_f64(h);
+    int r = mixed_to_staging(h);
+    if (r) return r;
+    r = do_sort_f64(h);
+    if (r) return r;
+    return mixed_from_staging(h);
+}
+
+int do_sort_f64(mpm_handle* h) {
     if (h->n == 0) return MPM_OK;
     int r = ensure_sort_scratch(h);
     if (r) return r;
@@ -300,7 +434,8 @@ mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity
     mpm_handle* h = nullptr;
     do {
         if (!params_valid(prms) || capacity == 0 ||
-            (precision != MPM_PRECISION_FP64 && precision != MPM_PRECISION_FP64_SVD64)) {
+            (precision != MPM_PRECISION_FP64 && precision != MPM_PRECISION_FP64_SVD64 &&
+             precision != MPM_PRECISION_MIXED)) {
             st = MPM_ERR_ARG;
             break;
         }
@@ -313,6 +448,10 @@ mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity
         cudaDeviceProp prop;
         if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) {
             st = MPM_ERR_NO_DEVICE;
+            break;
+        }
+        if ((long long)(prms->GridXTotal + 2 * prms->GridHaloSize) * prms->GridY * prms->GridZ >= 0x7fffffffLL) {
+            st = MPM_ERR_ARG;   // node indices are 32-bit in the kernels
             break;
         }
         h = new (std::nothrow) mpm_handle();
@@ -329,7 +468,9 @@ mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity
         if (cudaFuncSetAttribute(k_p2g_tile_f64<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(sizeof(double) * 4 * h->tile_cap)) != cudaSuccess ||
             cudaFuncSetAttribute(k_p2g_tile_f64<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(sizeof(double) * 4 * h->tile_cap)) != cudaSuccess) {
+                                 (int)(sizeof(double) * 4 * h->tile_cap)) != cudaSuccess ||
+            cudaFuncSetAttribute(k_p2g_fx_f64<kFxBlock, kFxPPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(long long) * 4 * h->fx_tile_cap)) != cudaSuccess) {
             st = MPM_ERR_CUDA;
             break;
         }
@@ -342,6 +483,17 @@ mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity
             cudaMalloc(&h->err, sizeof(int)) != cudaSuccess) {
             st = MPM_ERR_CUDA;
             break;
+        }
+        if (precision == MPM_PRECISION_MIXED) {
+            if (cudaMalloc(&h->mx, sizeof(float) * MPM_N_PTS_ARRAYS * h->pitch) != cudaSuccess ||
+                cudaMalloc(&h->gacc, sizeof(float4) * (size_t)h->dp.nodes) != cudaSuccess ||
+                cudaMalloc(&h->gvel, sizeof(float4) * (size_t)h->dp.nodes) != cudaSuccess) {
+                st = MPM_ERR_CUDA;
+                break;
+            }
+            cudaMemsetAsync(h->mx, 0, sizeof(float) * MPM_N_PTS_ARRAYS * h->pitch, h->stream);
+            cudaMemsetAsync(h->gacc, 0, sizeof(float4) * (size_t)h->dp.nodes, h->stream);
+            cudaMemsetAsync(h->gvel, 0, sizeof(float4) * (size_t)h->dp.nodes, h->stream);
         }
         cudaMemsetAsync(h->pts, 0, sizeof(double) * MPM_N_PTS_ARRAYS * h->pitch, h->stream);
         cudaMemsetAsync(h->grid, 0, sizeof(double) * 4 * (size_t)h->dp.gstride, h->stream);
@@ -380,6 +532,7 @@ int mpm_update_constants(mpm_handle* h, const SimParams3D* prms) {
         return MPM_ERR_ARG;
     h->prms = *prms;
     h->dp = make_dev_params(*prms);
+    h->p2g_ready = false;
     CK(h, cudaMemsetAsync(h->err, 0, sizeof(int), h->stream));
     return MPM_OK;
 }
@@ -397,6 +550,11 @@ int mpm_upload_soa(mpm_handle* h, const double* soa, unsigned pitch, unsigned n)
     }
     h->n = n;
     h->uploaded = true;
+    h->p2g_ready = false;
+    if (is_mixed(h)) {
+        int r = mixed_from_staging(h);
+        if (r) return r;
+    }
     CK(h, cudaMemsetAsync(h->err, 0, sizeof(int), h->stream));
     return MPM_OK;
 }
@@ -404,9 +562,13 @@ int mpm_upload_soa(mpm_handle* h, const double* soa, unsigned pitch, unsigned n)
 int mpm_upload_cohesion(mpm_handle* h, const double* c, unsigned n) {
     if (!h) return MPM_ERR_ARG;
     if (!c) {
+        cudaStreamSynchronize(h->stream);
         cudaFree(h->p0);
         cudaFree(h->p0_alt);
+        cudaFree(h->p0f);
         h->p0 = h->p0_alt = nullptr;
+        h->p0f = nullptr;
+        h->p2g_ready = false;
         return MPM_OK;
     }
     if (n != h->n || h->prms.DP_tan_phi == 0) return MPM_ERR_ARG;
@@ -415,11 +577,21 @@ int mpm_upload_cohesion(mpm_handle* h, const double* c, unsigned n) {
     for (unsigned i = 0; i < n; i++) p0[i] = c[i] / h->prms.DP_tan_phi;
     CK(h, cudaMemcpyAsync(h->p0, p0.data(), sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
+    h->p2g_ready = false;
+    if (is_mixed(h) && n) {
+        if (!h->p0f) CK(h, cudaMalloc(&h->p0f, sizeof(float) * h->pitch));
+        k_narrow<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->p0, h->p0f, (int)n);
+        CK_LAUNCH(h, "p0 narrow");
+    }
     return MPM_OK;
 }
 
 int mpm_download_soa(mpm_handle* h, double* soa, unsigned pitch, unsigned* n) {
     if (!h || !soa || pitch < h->n) return MPM_ERR_ARG;
+    if (is_mixed(h)) {
+        int r = mixed_to_staging(h);
+        if (r) return r;
+    }
     if (h->n) {
         CK(h, cudaMemcpy2DAsync(soa, sizeof(double) * pitch, h->pts, sizeof(double) * h->pitch, sizeof(double) * h->n,
                                 MPM_N_PTS_ARRAYS, cudaMemcpyDeviceToHost, h->stream));
@@ -463,17 +635,20 @@ int mpm_reset_grid(mpm_handle* h) {
 int mpm_p2g(mpm_handle* h) {
     if (!h) return MPM_ERR_ARG;
     if (!h->uploaded) return MPM_ERR_STATE;
+    h->p2g_ready = false;
     return launch_p2g(h);
 }
 
 int mpm_update_nodes(mpm_handle* h, double indenter_x, double indenter_y) {
     if (!h) return MPM_ERR_ARG;
+    h->p2g_ready = false;
     return launch_update(h, indenter_x, indenter_y, h->force_phase);
 }
 
 int mpm_g2p(mpm_handle* h, int record_pq) {
     if (!h) return MPM_ERR_ARG;
     if (!h->uploaded) return MPM_ERR_STATE;
+    h->p2g_ready = false;
     return launch_g2p(h, record_pq);
 }
 
@@ -496,10 +671,28 @@ int mpm_step(mpm_handle* h, int nsteps, double* force_hist) {
     }
     CK(h, cudaMemsetAsync(h->force_steps, 0, sizeof(double) * 3 * (size_t)nsteps, h->stream));
     SimParams3D& p = h->prms;
+    if (is_mixed(h) && !h->p2g_ready) {
+        int r;
+        if ((r = reset_grid(h))) return r;
+        if ((r = launch_p2g(h))) return r;
+        h->p2g_ready = true;
+    }
     for (int s = 0; s < nsteps; s++) {
         p.SimulationTime += p.InitialTimeStep;
         p.indenter_x = p.indenter_x_initial + p.SimulationTime * p.IndVelocity;
         int r;
+        if (is_mixed(h)) {
+            // node update of this substep, then G2P of this substep fused with
+            // the P2G of the next one (the accumulator stays ready)
+            if ((r = launch_update(h, p.indenter_x, p.indenter_y, h->force_steps + 3 * s))) return r;
+            const int record = (p.SimulationStep % p.UpdateEveryNthStep) == 0;
+            if ((r = launch_g2p2g_mixed(h, 1, record))) return r;
+            p.SimulationStep += 1;
+            if (h->sort_interval > 0 && ++h->steps_since_sort >= h->sort_interval) {
+                if ((r = do_sort(h))) return r;
+            }
+            continue;
+        }
         if ((r = reset_grid(h))) return r;
         if ((r = launch_p2g(h))) return r;
         if ((r = launch_update(h, p.indenter_x, p.indenter_y, h->force_steps + 3 * s))) return r;
@@ -619,9 +812,94 @@ int mpm_testing_svd3x3(int mode, const double* A, int count, double* U, double* 
 
 size_t mpm_testing_sizeof_params(void) { return sizeof(SimParams3D); }
 
-int mpm_testing_download_grid(mpm_handle* h, double* out) {
+int mpm_testing_step_timed(mpm_handle* h, int nsteps, float* ms) {
+    if (!h || nsteps <= 0 || !ms) return MPM_ERR_ARG;
+    if (!h->uploaded) return MPM_ERR_STATE;
+    cudaEvent_t ev[5];
+    for (int k = 0; k < 5; k++) CK(h, cudaEventCreate(&ev[k]));
+    for (int k = 0; k < 4; k++) ms[k] = 0.f;
+    SimParams3D& p = h->prms;
+    int r = MPM_OK;
+    if (is_mixed(h) && !h->p2g_ready) {
+        if ((r = reset_grid(h)) || (r = launch_p2g(h))) return r;
+        h->p2g_ready = true;
+    }
+    if (!h->force_phase) return MPM_ERR_STATE;
+    for (int s = 0; s < nsteps && !r; s++) {
+        p.SimulationTime += p.InitialTimeStep;
+        p.indenter_x = p.indenter_x_initial + p.SimulationTime * p.IndVelocity;
+        const int record = (p.SimulationStep % p.UpdateEveryNthStep) == 0;
+        cudaEventRecord(ev[0], h->stream);
+        if (is_mixed(h)) {
+            cudaEventRecord(ev[1], h->stream);
+            cudaEventRecord(ev[2], h->stream);
+            if ((r = launch_update(h, p.indenter_x, p.indenter_y, h->force_phase))) break;
+            cudaEventRecord(ev[3], h->stream);
+            if ((r = launch_g2p2g_mixed(h, 1, record))) break;
+        } else {
+            if ((r = reset_grid(h))) break;
+            cudaEventRecord(ev[1], h->stream);
+            if ((r = launch_p2g(h))) break;
+            cudaEventRecord(ev[2], h->stream);
+            if ((r = launch_update(h, p.indenter_x, p.indenter_y, h->force_phase))) break;
+            cudaEventRecord(ev[3], h->stream);
+            if ((r = launch_g2p(h, record))) break;
+        }
+        cudaEventRecord(ev[4], h->stream);
+        CK(h, cudaEventSynchronize(ev[4]));
+        for (int k = 0; k < 4; k++) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+            ms[k] += t;
+        }
+        p.SimulationStep += 1;
+    }
+    for (int k = 0; k < 5; k++) cudaEventDestroy(ev[k]);
+    return r;
+}
+
+int mpm_testing_active_nodes(mpm_handle* h, long long* count) {
+    if (!h || !count) return MPM_ERR_ARG;
+    const size_t nodes = (size_t)h->dp.nodes;
+    long long c = 0;
+    if (is_mixed(h)) {
+        std::vector<float4> g(nodes);
+        CK(h, cudaMemcpyAsync(g.data(), h->gacc, sizeof(float4) * nodes, cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        for (size_t i = 0; i < nodes; i++) c += g[i].x != 0.f;
+    } else {
+        std::vector<double> m(nodes);
+        CK(h, cudaMemcpyAsync(m.data(), h->grid, sizeof(double) * nodes, cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        for (size_t i = 0; i < nodes; i++) c += m[i] != 0.0;
+    }
+    *count = c;
+    return MPM_OK;
+}
+
+int mpm_testing_set_g2p_variant(mpm_handle* h, int variant) {
+    if (!h || variant < 0 || variant > 2) return MPM_ERR_ARG;
+    h->g2p_variant = variant;
+    h->mixed_variant = variant;
+    return MPM_OK;
+}
+
+int mpm_testing_download_grid(mpm_handle* h, double* out, int which) {
     if (!h || !out) return MPM_ERR_ARG;
     const size_t nodes = (size_t)h->dp.nodes;
+    if (is_mixed(h)) {
+        std::vector<float4> g(nodes);
+        CK(h, cudaMemcpyAsync(g.data(), which ? h->gvel : h->gacc, sizeof(float4) * nodes, cudaMemcpyDeviceToHost,
+                              h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        for (size_t i = 0; i < nodes; i++) {
+            out[i] = which ? 0.0 : g[i].x;
+            out[nodes + i] = which ? g[i].x : g[i].y;
+            out[2 * nodes + i] = which ? g[i].y : g[i].z;
+            out[3 * nodes + i] = which ? g[i].z : g[i].w;
+        }
+        return MPM_OK;
+    }
     for (int c = 0; c < 4; c++)
         CK(h, cudaMemcpyAsync(out + c * nodes, h->grid + c * h->dp.gstride, sizeof(double) * nodes,
                               cudaMemcpyDeviceToHost, h->stream));
@@ -630,7 +908,7 @@ int mpm_testing_download_grid(mpm_handle* h, double* out) {
 }
 
 int mpm_testing_set_p2g_variant(mpm_handle* h, int variant) {
-    if (!h || variant < 0 || variant > 3) return MPM_ERR_ARG;
+    if (!h || variant < 0 || variant > 4) return MPM_ERR_ARG;
     h->p2g_variant = variant;
     return MPM_OK;
 }

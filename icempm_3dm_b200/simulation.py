@@ -125,12 +125,25 @@ class MPMHandle:
     def reset_indenter_force_accumulator(self):
         check(LIB.mpm_reset_indenter_force_accumulator(self._h), "mpm_reset_indenter_force_accumulator")
 
-    def grid(self):
+    def grid(self, which=0):
         p = self.prms
         nodes = (p.GridXTotal + 2 * p.GridHaloSize) * p.GridY * p.GridZ
         g = np.zeros((4, nodes))
-        check(LIB.mpm_testing_download_grid(self._h, dptr(g)), "mpm_testing_download_grid")
+        check(LIB.mpm_testing_download_grid(self._h, dptr(g), which), "mpm_testing_download_grid")
         return g
+
+    def step_timed(self, nsteps):
+        ms = (ctypes.c_float * 4)()
+        check(LIB.mpm_testing_step_timed(self._h, nsteps, ms), "mpm_testing_step_timed")
+        return [ms[k] for k in range(4)]
+
+    def active_nodes(self):
+        c = ctypes.c_longlong(0)
+        check(LIB.mpm_testing_active_nodes(self._h, ctypes.byref(c)), "mpm_testing_active_nodes")
+        return c.value
+
+    def set_g2p_variant(self, v):
+        check(LIB.mpm_testing_set_g2p_variant(self._h, v), "mpm_testing_set_g2p_variant")
 
     def set_p2g_variant(self, v):
         check(LIB.mpm_testing_set_p2g_variant(self._h, v), "mpm_testing_set_p2g_variant")

@@ -12,11 +12,17 @@
 extern "C" {
 #endif
 
-/* P2G kernel of the phase API and of mpm_step: 0 = shared-memory tile with
- * one flush per tile node (default), 1 = one thread per particle with 27x4
+/* P2G kernel of the phase API and of mpm_step: 0 = shared-memory FP64 tile
+ * with one flush per tile node, 1 = one thread per particle with 27x4
  * global atomics, 2 = as 1 with a warp reduction over particles sharing a
- * base cell, 3 = as 0 with that warp reduction. */
+ * base cell, 3 = as 0 with that warp reduction, 4 = shared-memory tile in
+ * 64-bit block fixed point over 1024-particle chunks (default). */
 int mpm_testing_set_p2g_variant(mpm_handle* h, int variant);
+
+/* G2P kernel occupancy target (FP64 modes): 0 = 4 blocks of 128 threads per
+ * SM, 1 = 3 blocks, 2 = 6 blocks (default; fewer registers per thread). In
+ * the mixed mode the fused kernel's target: 0 = 4, 1 = 5, 2 = 6 blocks. */
+int mpm_testing_set_g2p_variant(mpm_handle* h, int variant);
 
 /* Runs the device 3x3 SVD on `count` row-major matrices A (9 doubles each)
  * on `device`: mode 0 = FP32 arithmetic of the reference, mode 1 = FP64.
@@ -25,8 +31,21 @@ int mpm_testing_svd3x3(int mode, const double* A, int count, double* U, double* 
 
 /* Copies the grid to the host as 4 rows [m, mvx|vx, mvy|vy, mvz|vz] of
  * (GridXTotal + 2*GridHaloSize)*GridY*GridZ doubles, node order
- * ((x + halo)*GridY + y)*GridZ + z (the reference's one-partition buffer). */
-int mpm_testing_download_grid(mpm_handle* h, double* out);
+ * ((x + halo)*GridY + y)*GridZ + z (the reference's one-partition buffer).
+ * FP64 modes keep one grid (which is ignored); the mixed mode keeps the
+ * accumulator (which = 0: m, m v) and the updated velocities (which = 1:
+ * 0, v) apart. */
+int mpm_testing_download_grid(mpm_handle* h, double* out, int which);
+
+/* Runs nsteps substeps like mpm_step (without the force history) with CUDA
+ * events recorded on the handle's stream around each kernel; ms[0..3]
+ * receive the summed durations of [grid clear, P2G, node update, G2P] (FP64
+ * modes) or [-, -, node update, fused G2P->P2G] (mixed mode). */
+int mpm_testing_step_timed(mpm_handle* h, int nsteps, float* ms);
+
+/* Number of grid nodes with non-zero mass in the current P2G result (the
+ * accumulator in mixed mode; the grid after P2G in FP64 modes). */
+int mpm_testing_active_nodes(mpm_handle* h, long long* count);
 
 /* sizeof(SimParams3D) as compiled into the library (layout check). */
 size_t mpm_testing_sizeof_params(void);

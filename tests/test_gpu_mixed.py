@@ -1,0 +1,104 @@
+"""GPU parity of the mixed-precision step (FP32 state and transfers, FP64
+SVD / return map / force reduction) against the FP64 oracle with the FP64
+SVD variant, through the C-ABI.
+
+Tolerances (FP32 arithmetic): per-field single-step relative deviation
+<= 2e-5 of the field's magnitude, positions <= 1e-7 m absolute; the
+indenter force history over 60 substeps within 1e-3 relative (the north
+star's bound for the mixed form).
+"""
+import numpy as np
+import pytest
+
+from icempm_3dm_b200 import MPMHandle, PRECISION_MIXED
+from icempm_3dm_b200._lib import BP00, FE00, IDX_JP_INV, IDX_UTILITY, POSX, STATUS_CRUSHED, VELX
+from oracle import pyoracle as po
+from tests.helpers import perturbed_block, util_bits
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_dev(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.abs(b).max(), 1e-300))
+
+
+def test_upload_download_round_trip():
+    prms, soa = perturbed_block(n=3000, seed=71)
+    with MPMHandle(prms, soa.shape[1], PRECISION_MIXED) as h:
+        h.upload(soa)
+        out = h.download()
+    assert np.abs(out[POSX:POSX + 3] - soa[POSX:POSX + 3]).max() < 2e-8
+    assert rel_dev(out[VELX:VELX + 3], soa[VELX:VELX + 3]) < 1e-7
+    assert np.abs(out[FE00:FE00 + 9] - soa[FE00:FE00 + 9]).max() < 1e-8
+    assert rel_dev(out[BP00:BP00 + 9], soa[BP00:BP00 + 9]) < 1e-7
+    assert np.array_equal(util_bits(out), util_bits(soa))
+
+
+def test_single_step_phases_close_to_oracle():
+    prms, soa = perturbed_block(n=4000, seed=31)
+    n = soa.shape[1]
+    ix = prms.indenter_x + 0.02
+    with MPMHandle(prms, n, PRECISION_MIXED) as h:
+        h.upload(soa)
+        h.reset_indenter_force_accumulator()
+        h.reset_grid()
+        h.p2g()
+        acc = h.grid(0)
+        h.update_nodes(ix, prms.indenter_y)
+        vel = h.grid(1)
+        h.g2p(True)
+        out = h.download()
+    ref_grid, _ = po.p2g(prms, soa, n)
+    assert rel_dev(acc[0], ref_grid[0]) < 1e-6
+    for c in range(1, 4):
+        assert rel_dev(acc[c], ref_grid[c]) < 2e-5, c
+    mass = ref_grid[0].copy()
+    po.update_nodes(prms, ref_grid, ix, prms.indenter_y)
+    live = mass > 1e-3 * mass.max()
+    for c in range(1, 4):
+        assert rel_dev(vel[c][live], ref_grid[c][live]) < 2e-5, c
+    ref = soa.copy()
+    po.g2p(prms, ref, n, ref_grid, record_pq=True, svd_mode=1)
+    crushed_ref = (util_bits(ref) & STATUS_CRUSHED) != 0
+    crushed = (util_bits(out) & STATUS_CRUSHED) != 0
+    assert np.mean(crushed != crushed_ref) < 1e-3
+    same = crushed == crushed_ref
+    assert np.abs(out[POSX:POSX + 3] - ref[POSX:POSX + 3]).max() < 1e-7
+    assert rel_dev(out[VELX:VELX + 3], ref[VELX:VELX + 3]) < 2e-5
+    assert rel_dev(out[BP00:BP00 + 9], ref[BP00:BP00 + 9]) < 2e-5
+    dF = np.abs(out[FE00:FE00 + 9][:, same] - ref[FE00:FE00 + 9][:, same]).max()
+    assert dF < 2e-6, dF
+    assert rel_dev(out[IDX_JP_INV][same], ref[IDX_JP_INV][same]) < 1e-5
+
+
+def test_force_history_within_1e3_of_fp64():
+    prms, soa = perturbed_block(n=3000, seed=41, ind_velocity=0.5, crushed_frac=0.05, strong_frac=0.0)
+    n = soa.shape[1]
+    steps = 60
+    with MPMHandle(prms, n, PRECISION_MIXED) as h:
+        h.upload(soa)
+        hist = h.step(steps)
+        out = h.download()
+    sim = po.OracleSim(prms, soa, n, svd_mode=1)
+    ref_hist, err = sim.step(steps)
+    assert err == 0
+    norm = np.linalg.norm(ref_hist)
+    assert norm > 0
+    assert np.linalg.norm(hist - ref_hist) / norm < 1e-3
+    assert np.abs(out[POSX:POSX + 3] - sim.soa[POSX:POSX + 3]).max() < 1e-6
+
+
+def test_sort_in_mixed_mode_matches_oracle_permutation():
+    prms, soa = perturbed_block(n=4000, seed=81)
+    n = soa.shape[1]
+    rng = np.random.default_rng(2)
+    soa = np.ascontiguousarray(soa[:, rng.permutation(n)])
+    with MPMHandle(prms, n, PRECISION_MIXED) as h:
+        h.upload(soa)
+        held = h.download()          # positions as the mixed state holds them
+        h.sort()
+        ids = h.ids()
+        out = h.download()
+    perm = po.sort_permutation(prms, held, n)
+    assert np.array_equal(ids, perm)
+    assert np.array_equal(out, held[:, perm])
