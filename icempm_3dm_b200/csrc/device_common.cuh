@@ -29,6 +29,8 @@ struct DevParams {
     double pmax, tensile, shear, tensile2, beta, grain_var;
     double tan_phi, p0;            // DP_tan_phi, DP_threshold_p
     double drag;
+    // failure-surface constants for GrainVariability = 0 (FP32 fast path)
+    float fs_pmin2, fs_k, fs_msq, fs_1p2b, fs_bpmax, fs_pmax;
 };
 
 constexpr double kCoeff1 = 1.224744871391589;      // sqrt(3/2)

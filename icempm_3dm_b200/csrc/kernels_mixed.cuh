@@ -72,6 +72,53 @@ __device__ __forceinline__ void dev_b(const float E[3][3], float D[3][3]) {
     D[0][0] -= t; D[1][1] -= t; D[2][2] -= t;
 }
 
+// J - 1, J, J^(-2/3) and dev(F F^T) of F = I + E: shared by the trial p, q
+// (mpm_kernels.cuh:477-484) and the Kirchhoff stress (:547-557)
+struct ElasticInv {
+    float jm1, J, jm23;
+    float D[3][3];
+};
+
+__device__ __forceinline__ ElasticInv elastic_invariants(const float E[3][3]) {
+    ElasticInv e;
+    e.jm1 = detm1(E);
+    e.J = 1.0f + e.jm1;
+    e.jm23 = exp2f(-(2.0f / 3.0f) * log2f(e.J));
+    dev_b(E, e.D);
+    return e;
+}
+
+__device__ __forceinline__ void trial_pq_inv(const DevParams& P, const ElasticInv& e, float& p_tr, float& q_tr) {
+    p_tr = -(float)(0.5 * P.kappa) * (e.jm1 * (e.J + 1.0f));
+    float sq = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) sq += e.D[i][j] * e.D[i][j];
+    q_tr = (float)(kCoeff1 * P.mu) * e.jm23 * sqrtf(sq);
+}
+
+__device__ __forceinline__ void tau_inv(const DevParams& P, const ElasticInv& e, float tau[3][3]) {
+    const float s = (float)P.mu * e.jm23;
+    const float hyd = (float)(P.kappa * 0.5) * (e.jm1 * (e.J + 1.0f));
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) tau[i][j] = s * e.D[i][j] + (i == j ? hyd : 0.0f);
+}
+
+// CheckIfPointIsInsideFailureSurface (mpm_kernels.cuh:453-474) in FP32; the
+// grain-independent constants come precomputed when GrainVariability = 0.
+__device__ __forceinline__ bool outside_failure_surface_f32(const DevParams& P, short grain, float p_tr, float q_tr) {
+    if (P.grain_var != 0.0) return outside_failure_surface(P, grain, (double)p_tr, (double)q_tr);
+    if (p_tr < 0.f) {
+        if (p_tr < P.fs_pmin2) return true;
+        return q_tr > P.fs_k * (p_tr - P.fs_pmin2);
+    }
+    const float y = P.fs_1p2b * q_tr * q_tr + P.fs_msq * (p_tr + P.fs_bpmax) * (p_tr - P.fs_pmax);
+    return y > 0.f;
+}
+
 // Kirchhoff stress (mpm_kernels.cuh:547-557) from E
 __device__ __forceinline__ void kirchhoff_mixed(const DevParams& P, const float E[3][3], float tau[3][3]) {
     const float jm1 = detm1(E);
@@ -149,36 +196,46 @@ __device__ __forceinline__ void g2p_gather_mixed(const DevParams& P, const float
     }
 }
 
-// Return map of a crushed point in FP64 (mpm_kernels.cuh:486-544), E in/out.
-__device__ __noinline__ void return_map_f64(const DevParams& P, float E[3][3], float& Jp, double p0) {
+// Return map of a crushed point in FP64 (mpm_kernels.cuh:486-544). Out of
+// line (it is rare and register-hungry); arguments and result travel by
+// value so that nothing of the caller is forced into local memory.
+struct ElasticState {
+    float e[9];   // F - I, row-major
+    float jp;     // Jp_inv
+};
+
+__device__ __noinline__ ElasticState return_map_f64(const DPParams P, const ElasticState in, const double p0) {
     double F[3][3];
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-        for (int j = 0; j < 3; j++) F[i][j] = (i == j ? 1.0 : 0.0) + (double)E[i][j];
+        for (int j = 0; j < 3; j++) F[i][j] = (i == j ? 1.0 : 0.0) + (double)in.e[3 * i + j];
     double Je, p_tr, q_tr;
     trial_pq(P, F, Je, p_tr, q_tr);
-    double jp = Jp;
+    double jp = in.jp;
     drucker_prager_return<SvdF64>(P, F, jp, Je, p_tr, q_tr, p0);
-    Jp = (float)jp;
+    ElasticState out;
+    out.jp = (float)jp;
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-        for (int j = 0; j < 3; j++) E[i][j] = (float)(F[i][j] - (i == j ? 1.0 : 0.0));
+        for (int j = 0; j < 3; j++) out.e[3 * i + j] = (float)(F[i][j] - (i == j ? 1.0 : 0.0));
+    return out;
 }
 
 // ------------------------------------------------------------- P2G part
 
 // Scatter of one particle (base, fx, m, mv, S) with the warp reduction over
 // lanes sharing a base cell; leaders add float4 {m, mv} to acc.
+template <bool AGG = true>
 __device__ __forceinline__ void p2g_scatter_mixed(const DevParams& P, float4* __restrict__ acc, bool active, bool inside,
                                                   const int base[3], const float fx[3], float mass, const float mv[3],
                                                   const float S[3][3], int lane) {
     const int i0 = ((base[0] + P.halo) * P.Gy + base[1]) * P.Gz + base[2];
     const int key = inside ? i0 : -1 - lane;
-    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const unsigned peers = AGG ? __match_any_sync(0xffffffffu, key) : (1u << lane);
     const int leader = __ffs(peers) - 1;
-    const int rounds = (int)__reduce_max_sync(0xffffffffu, (unsigned)(__popc(peers) - 1));
+    const int rounds = AGG ? (int)__reduce_max_sync(0xffffffffu, (unsigned)(__popc(peers) - 1)) : 0;
     float ww[3][3];
     quad_weights<float>(fx, ww);
     const float h = (float)P.h;
@@ -216,6 +273,84 @@ __device__ __forceinline__ void p2g_scatter_mixed(const DevParams& P, float4* __
             }
         }
     }
+}
+
+// Shared-memory tile variant of the scatter. The block's particles (a
+// contiguous range of the cell-sorted order) span a small box of nodes; the
+// block accumulates the box with FP32 shared-memory atomics and adds each non-empty node to the grid once, as one
+// float4 vector atomic. Returns false (nothing done) when the box exceeds the
+// tile; the caller then scatters directly. Must be called by the whole block.
+template <int BLOCK>
+__device__ __forceinline__ bool p2g_scatter_tile(const DevParams& P, float4* __restrict__ acc, float* __restrict__ tile,
+                                                 int tile_cap, bool active, bool inside, const int base[3],
+                                                 const float fx[3], float mass, const float mv[3], const float S[3][3],
+                                                 int lane) {
+    __shared__ int s_box[6];
+    if (threadIdx.x < 3) { s_box[threadIdx.x] = INT_MAX; s_box[3 + threadIdx.x] = INT_MIN; }
+    __syncthreads();
+    const bool in_box = active && inside;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        int lo = in_box ? base[d] : INT_MAX, hi = in_box ? base[d] + 2 : INT_MIN;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if (lane == 0) { atomicMin(&s_box[d], lo); atomicMax(&s_box[3 + d], hi); }
+    }
+    __syncthreads();
+    const int bx = s_box[0], by = s_box[1], bz = s_box[2];
+    const int ex = s_box[3] - bx + 1, ey = s_box[4] - by + 1, ez = s_box[5] - bz + 1;
+    if (bx > s_box[3]) return true;   // no particle of the block is inside
+    const long long vol = (long long)ex * ey * ez;
+    if (vol > tile_cap) return false;
+    const int nv = (int)vol;
+    for (int k = threadIdx.x; k < 4 * nv; k += BLOCK) tile[k] = 0.f;
+    __syncthreads();
+    // particles of the block whose stencil leaves the grid go direct
+    if (active && !inside) {
+        p2g_scatter_mixed<false>(P, acc, active, inside, base, fx, mass, mv, S, lane);
+    } else {
+        const int t0 = ((base[0] - bx) * ey + (base[1] - by)) * ez + (base[2] - bz);
+        float ww[3][3];
+        quad_weights<float>(fx, ww);
+        const float h = (float)P.h;
+#pragma unroll 1
+        for (int a = 0; a < 3; a++) {
+            const float dx = (a - fx[0]) * h;
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                const float dy = (b - fx[1]) * h;
+                const float wab = ww[a][0] * ww[b][1];
+                const int tb = t0 + (a * ey + b) * ez;
+                float part[3];
+#pragma unroll
+                for (int m = 0; m < 3; m++) part[m] = mv[m] + S[m][0] * dx + S[m][1] * dy;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const float dz = (c - fx[2]) * h;
+                    const float W = wab * ww[c][2];
+                    if (!in_box) continue;
+                    const int t = tb + c;
+                    atomicAdd(tile + t, W * mass);
+                    atomicAdd(tile + nv + t, W * (part[0] + S[0][2] * dz));
+                    atomicAdd(tile + 2 * nv + t, W * (part[1] + S[1][2] * dz));
+                    atomicAdd(tile + 3 * nv + t, W * (part[2] + S[2][2] * dz));
+                }
+            }
+        }
+    }
+    __syncthreads();
+    const int slab = (int)P.slab, gz = P.Gz;
+    const int g0 = ((bx + P.halo) * P.Gy + by) * gz + bz;
+    for (int t = threadIdx.x; t < nv; t += BLOCK) {
+        const float m = tile[t];
+        if (m == 0.f) continue;
+        const int tz = t % ez, ty = (t / ez) % ey, tx = t / (ez * ey);
+        atomicAdd(acc + (g0 + tx * slab + ty * gz + tz), make_float4(m, tile[nv + t], tile[2 * nv + t], tile[3 * nv + t]));
+    }
+    return true;
 }
 
 // P2G payload of a particle: S = m C - dt V Dp^-1 tau (mpm_kernels.cuh:63)
@@ -290,10 +425,13 @@ __global__ void __launch_bounds__(256) k_p2g_mixed(DevParams P, MixedState s, in
 }
 
 // Fused G2P (this step) -> P2G (next step). do_p2g = 0 gives a plain G2P.
-template <int MINB>
+// SCATTER: 0 = warp-reduced direct float4 atomics, 1 = direct float4
+// atomics, 2 = shared-memory tile (falls back to 0 when the box is too big)
+template <int MINB, int SCATTER>
 __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedState s, int n,
                                                            const float4* __restrict__ vel, float4* __restrict__ acc,
-                                                           int do_p2g, int record_pq, int* err) {
+                                                           int do_p2g, int record_pq, int* err, int tile_cap) {
+    extern __shared__ float mixed_tile[];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     bool active = i < n;
@@ -305,6 +443,7 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     int base[3];
     float fx[3], v[3] = {0, 0, 0}, C[3][3];
     bool inside = false;
+    ElasticInv inv;
     if (active) {
 #pragma unroll
         for (int d = 0; d < 3; d++) fix_base(X[d], base[d], fx[d]);
@@ -340,13 +479,20 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
             for (int r = 0; r < 3; r++)
 #pragma unroll
                 for (int c = 0; c < 3; c++) E[r][c] = En[r][c];
-            float jm1;
-            trial_pq_mixed(P, E, jm1, p_tr, q_tr);
-            if (!(st & (int)kCrushed) && outside_failure_surface(P, (short)st, (double)p_tr, (double)q_tr))
-                st |= (int)kCrushed;
+            inv = elastic_invariants(E);
+            trial_pq_inv(P, inv, p_tr, q_tr);
+            if (!(st & (int)kCrushed) && outside_failure_surface_f32(P, (short)st, p_tr, q_tr)) st |= (int)kCrushed;
             if (st & (int)kCrushed) {
                 const double p0 = s.p0 ? (double)s.p0[i] : P.p0;
-                return_map_f64(P, E, Jp, p0);
+                ElasticState es;
+#pragma unroll
+                for (int k = 0; k < 9; k++) es.e[k] = E[k / 3][k % 3];
+                es.jp = Jp;
+                es = return_map_f64(dp_params(P), es, p0);
+#pragma unroll
+                for (int k = 0; k < 9; k++) E[k / 3][k % 3] = es.e[k];
+                Jp = es.jp;
+                inv = elastic_invariants(E);
             }
         }
         // store state
@@ -374,7 +520,20 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     if (active) {
 #pragma unroll
         for (int d = 0; d < 3; d++) fix_base(X[d], base[d], fx[d]);
-        p2g_payload_mixed(P, E, C, v, (st & (int)kLiquid) != 0, Jp, mass, mv, S);
+        if (st & (int)kLiquid) {
+            p2g_payload_mixed(P, E, C, v, true, Jp, mass, mv, S);
+        } else {
+            mass = (float)P.particle_mass;
+            float tau[3][3];
+            tau_inv(P, inv, tau);
+            const float dvd = (float)P.dt_vol_Dpinv;
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                mv[r] = v[r] * mass;
+#pragma unroll
+                for (int c = 0; c < 3; c++) S[r][c] = mass * C[r][c] - dvd * tau[r][c];
+            }
+        }
         const int e = stencil_error(P, base[0], base[1], base[2]);
         if (e) raise_error(err, e);
         inside = e == 0;
@@ -386,7 +545,10 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
 #pragma unroll
             for (int c = 0; c < 3; c++) S[r][c] = 0.f;
     }
-    p2g_scatter_mixed(P, acc, active, inside, base, fx, mass, mv, S, lane);
+    if (SCATTER == 2 && p2g_scatter_tile<128>(P, acc, mixed_tile, tile_cap, active, inside, base, fx, mass, mv, S, lane))
+        return;
+    if (SCATTER == 1) p2g_scatter_mixed<false>(P, acc, active, inside, base, fx, mass, mv, S, lane);
+    else p2g_scatter_mixed<true>(P, acc, active, inside, base, fx, mass, mv, S, lane);
 }
 
 // Node update for the mixed grid: FP64 arithmetic on the FP32 sums, contact

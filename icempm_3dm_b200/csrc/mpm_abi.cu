@@ -6,6 +6,7 @@
 // and GPU_Implementation6 (gpu_implementation6.cpp); the kernels are in the
 // kernels_*.cuh / sort.cuh headers.
 
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -28,6 +29,7 @@ __global__ void k_narrow(const double* __restrict__ src, float* __restrict__ dst
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = (float)src[i];
 }
+constexpr int kMixedTileNodes = 2048;   // 32 KB FP32 tile of the fused mixed kernel
 constexpr int kFxBlock = 256;   // threads of the fixed-point P2G
 constexpr int kFxPPT = 4;       // particles per thread (1024-particle chunks)
 }  // namespace
@@ -75,7 +77,8 @@ struct mpm_handle {
     float4* gacc = nullptr;
     float4* gvel = nullptr;
     bool p2g_ready = false;           // gacc holds the P2G of the current state
-    int mixed_variant = 0;            // fused kernel occupancy target (test hook)
+    int mixed_variant = 2;            // fused kernel occupancy target (test hook)
+    int mixed_scatter = 1;            // fused kernel scatter: 0 warp-reduced, 1 direct (default), 2 tile (test hook)
 
     int p2g_variant = 2;              // see mpm_testing_set_p2g_variant
     int g2p_variant = 2;              // see mpm_testing_set_g2p_variant
@@ -142,6 +145,17 @@ DevParams make_dev_params(const SimParams3D& p) {
     d.tan_phi = p.DP_tan_phi;
     d.p0 = p.DP_threshold_p;
     d.drag = p.DragGlobal;
+    {   // GetParametersForGrain with var2 = var3 = 1 (mpm_kernels.cuh:434-450)
+        const double pmax = p.IceCompressiveStrength, pmin = -p.IceTensileStrength, qmax = p.IceShearStrength;
+        const double pmin2 = -p.IceTensileStrength2, beta = p.NACC_beta;
+        const double q0 = 2 * std::sqrt(-pmax * pmin) * qmax / (pmax - pmin);
+        d.fs_pmin2 = (float)pmin2;
+        d.fs_k = (float)(-q0 / pmin2);
+        d.fs_msq = (float)((4 * qmax * qmax * (1 + 2 * beta)) / ((pmax - pmin) * (pmax - pmin)));
+        d.fs_1p2b = (float)(1. + 2. * beta);
+        d.fs_bpmax = (float)(beta * pmax);
+        d.fs_pmax = (float)pmax;
+    }
     return d;
 }
 
@@ -269,15 +283,19 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq) {
     const int n = (int)h->n;
     if (n == 0) return MPM_OK;
     const unsigned nb = blocks_for(n, 128);
-    if (h->mixed_variant == 1)
-        k_g2p2g_mixed<5><<<nb, 128, 0, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g, record_pq,
-                                                    h->err);
-    else if (h->mixed_variant == 2)
-        k_g2p2g_mixed<6><<<nb, 128, 0, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g, record_pq,
-                                                    h->err);
-    else
-        k_g2p2g_mixed<4><<<nb, 128, 0, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g, record_pq,
-                                                    h->err);
+    const size_t tsm = h->mixed_scatter == 2 ? sizeof(float) * 4 * kMixedTileNodes : 0;
+#define FUSED(MINB, SC)                                                                                          \
+    k_g2p2g_mixed<MINB, SC><<<nb, 128, tsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,     \
+                                                         record_pq, h->err, kMixedTileNodes)
+#define FUSED_SC(MINB)                              \
+    if (h->mixed_scatter == 2) FUSED(MINB, 2);      \
+    else if (h->mixed_scatter == 1) FUSED(MINB, 1); \
+    else FUSED(MINB, 0);
+    if (h->mixed_variant == 1) { FUSED_SC(5) }
+    else if (h->mixed_variant == 2) { FUSED_SC(6) }
+    else { FUSED_SC(4) }
+#undef FUSED_SC
+#undef FUSED
     CK_LAUNCH(h, "g2p2g mixed");
     return MPM_OK;
 }
@@ -908,7 +926,11 @@ int mpm_testing_download_grid(mpm_handle* h, double* out, int which) {
 }
 
 int mpm_testing_set_p2g_variant(mpm_handle* h, int variant) {
-    if (!h || variant < 0 || variant > 4) return MPM_ERR_ARG;
+    if (!h || variant < 0 || variant > 7) return MPM_ERR_ARG;
+    if (variant >= 5) {
+        h->mixed_scatter = variant - 5;
+        return MPM_OK;
+    }
     h->p2g_variant = variant;
     return MPM_OK;
 }

@@ -43,8 +43,9 @@ __device__ __forceinline__ double water_pressure(const DevParams& P, double J) {
     return P.kappa * (1. - pow(J, -3.0));
 }
 
-// ComputePQ (mpm_kernels.cuh:477-484)
-__device__ __forceinline__ void trial_pq(const DevParams& P, const double F[3][3], double& Je, double& p_tr,
+// ComputePQ (mpm_kernels.cuh:477-484); PP: DevParams or DPParams
+template <class PP>
+__device__ __forceinline__ void trial_pq(const PP& P, const double F[3][3], double& Je, double& p_tr,
                                          double& q_tr) {
     Je = det3(F);
     double Jsq = Je * Je;
@@ -97,8 +98,20 @@ __device__ __forceinline__ void compose_usv(const double U[3][3], const double d
 // ComputeSVD (mpm_kernels.cuh:486-492) + Wolper_Drucker_Prager (:494-544)
 // for a crushed point. p0 is the apex shift (DP_threshold_p, or the
 // per-particle cohesion / tan(phi)). K selects the SVD arithmetic.
-template <class K>
-__device__ __forceinline__ void drucker_prager_return(const DevParams& P, double F[3][3], double& Jp_inv,
+// The material constants the return map reads (a small by-value copy for
+// out-of-line callers).
+struct DPParams {
+    double mu, kappa, pmax, tensile, shear, tan_phi;
+};
+
+__device__ __forceinline__ DPParams dp_params(const DevParams& P) {
+    DPParams d;
+    d.mu = P.mu; d.kappa = P.kappa; d.pmax = P.pmax; d.tensile = P.tensile; d.shear = P.shear; d.tan_phi = P.tan_phi;
+    return d;
+}
+
+template <class K, class PP>
+__device__ __forceinline__ void drucker_prager_return(const PP& P, double F[3][3], double& Jp_inv,
                                                       double Je_tr, double p_tr, double q_tr, double p0) {
     typedef typename K::T T;
     T A[3][3], Uk[3][3], Sk[3], Vk[3][3];
