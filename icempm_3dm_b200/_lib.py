@@ -30,7 +30,7 @@ ERR_NAMES = {
     100: "CUDA runtime error", 101: "invalid argument", 102: "capacity exceeded", 103: "no suitable CUDA device",
     104: "configuration file not found", 105: "configuration file is not JSON / wrong key type",
     106: "config parameter missing (InputRawPoints)", 107: "cell key outside the grid",
-    108: "call out of order",
+    108: "call out of order", 109: "size beyond the fixed scratch of the allocation-free sort",
 }
 
 
@@ -128,6 +128,8 @@ ENTRY_POINTS = [
     ("mpm_get_params", ctypes.c_int, [_hp, _pp]),
     ("mpm_count", ctypes.c_int, [_hp, _up]),
     ("mpm_last_error_string", ctypes.c_char_p, []),
+    ("mpm_sort_permutation_noalloc", ctypes.c_int,
+     [_pp, ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p, _up, ctypes.c_void_p]),
     ("mpm_testing_set_p2g_variant", ctypes.c_int, [_hp, ctypes.c_int]),
     ("mpm_testing_set_g2p_variant", ctypes.c_int, [_hp, ctypes.c_int]),
     ("mpm_testing_svd3x3", ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int]),

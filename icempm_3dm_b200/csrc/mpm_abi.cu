@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -936,3 +937,103 @@ int mpm_testing_set_p2g_variant(mpm_handle* h, int variant) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------- sort without device allocation
+//
+// Some callers cannot let a library allocate device memory: applications that
+// own and budget every byte of the GPU themselves (their own pool, a fixed
+// footprint planned at start-up), and loops that cannot afford the latency
+// and implicit device-wide synchronisation of a cudaMalloc in the middle of a
+// run. mpm_sort_permutation_noalloc serves them: the caller passes its own
+// device buffers for input and output, and the sort's scratch lives in the
+// fixed array below, which every GPU that loads this library holds until the
+// process exits (about 10 MB).
+
+namespace {
+
+constexpr unsigned kNoAllocMaxParticles = 1u << 19;   // 524,288 particles
+constexpr unsigned kNoAllocMaxCells = 1u << 20;       // 1,048,576 cell keys incl. the disabled bucket
+constexpr unsigned kNoAllocTiles = kNoAllocMaxCells / kScanTile;
+// layout (ints): bucket[P] | count[C] | start[C] | tile sums[T] | tile scan[T] | error flag
+constexpr size_t kNoAllocOffCount = kNoAllocMaxParticles;
+constexpr size_t kNoAllocOffStart = kNoAllocOffCount + kNoAllocMaxCells;
+constexpr size_t kNoAllocOffSums = kNoAllocOffStart + kNoAllocMaxCells;
+constexpr size_t kNoAllocOffScan = kNoAllocOffSums + kNoAllocTiles;
+constexpr size_t kNoAllocOffErr = kNoAllocOffScan + kNoAllocTiles;
+constexpr size_t kNoAllocInts = kNoAllocOffErr + 64;
+static_assert(kNoAllocTiles <= (unsigned)kScanTile, "one scan level above the tiles");
+
+static __device__ __align__(256) int g_noalloc_sort_scratch[kNoAllocInts];
+
+// Device address of the scratch array per device: looked up once per device
+// (with that device current) on the first call made there.
+int* noalloc_scratch_for(int device, int* status) {
+    static std::mutex mu;
+    static int* ptrs[256] = {};
+    if (device < 0 || device >= 256) { *status = MPM_ERR_ARG; return nullptr; }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptrs[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_sort_scratch);
+        if (e != cudaSuccess) {
+            *status = cuda_fail(nullptr, e, "cudaGetSymbolAddress(sort scratch)");
+            return nullptr;
+        }
+        ptrs[device] = static_cast<int*>(p);
+    }
+    *status = MPM_OK;
+    return ptrs[device];
+}
+
+}  // namespace
+
+extern "C" int mpm_sort_permutation_noalloc(const SimParams3D* prms, const double* soa, unsigned pitch, unsigned n,
+                                            unsigned* perm, unsigned* kept, void* stream) {
+    if (!params_valid(prms) || (!soa && n) || (!perm && n) || !kept || pitch < n) return MPM_ERR_ARG;
+    const long long nb = (long long)(prms->GridXTotal + 2 * prms->GridHaloSize + 1) * prms->GridY * prms->GridZ;
+    if (n > kNoAllocMaxParticles || nb + 1 > (long long)kNoAllocMaxCells) return MPM_ERR_NOALLOC_LIMIT;
+    int dev = 0;
+    CK(nullptr, cudaGetDevice(&dev));
+    int st = MPM_OK;
+    int* scratch = noalloc_scratch_for(dev, &st);
+    if (!scratch) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int* bucket = scratch;
+    int* count = scratch + kNoAllocOffCount;
+    int* start = scratch + kNoAllocOffStart;
+    int* sums = scratch + kNoAllocOffSums;
+    int* scan = scratch + kNoAllocOffScan;
+    int* err = scratch + kNoAllocOffErr;
+    // the array keeps the previous call's contents: clear what is summed into
+    const int nb1 = (int)nb + 1;
+    CK(nullptr, cudaMemsetAsync(count, 0, sizeof(int) * nb1, s));
+    CK(nullptr, cudaMemsetAsync(err, 0, sizeof(int), s));
+    if (n) {
+        SortGeom G;
+        G.slab = prms->GridY * prms->GridZ;
+        G.gz = prms->GridZ;
+        G.key_shift = prms->GridHaloSize * G.slab;
+        G.nb = (int)nb;
+        G.h_inv = prms->cellsize_inv;
+        k_sort_keys<<<blocks_for(n, 256), 256, 0, s>>>(G, soa, pitch, (int)n, bucket, count, err);
+        CK_LAUNCH(nullptr, "noalloc sort keys");
+        const int tiles = (nb1 + kScanTile - 1) / kScanTile;
+        k_scan_tiles<<<tiles, kScanBlock, 0, s>>>(count, start, nb1, tiles > 1 ? sums : nullptr);
+        CK_LAUNCH(nullptr, "noalloc scan");
+        if (tiles > 1) {
+            k_scan_tiles<<<1, kScanBlock, 0, s>>>(sums, scan, tiles, nullptr);
+            k_scan_add<<<blocks_for(nb1, 256), 256, 0, s>>>(start, nb1, scan);
+            CK_LAUNCH(nullptr, "noalloc scan add");
+        }
+        CK(nullptr, cudaMemsetAsync(count, 0, sizeof(int) * nb1, s));
+        k_sort_scatter<<<blocks_for(n, 256), 256, 0, s>>>(bucket, (int)n, start, count, perm);
+        k_sort_fix<<<blocks_for(nb, 256), 256, 0, s>>>((int)nb, start, count, perm);
+        CK_LAUNCH(nullptr, "noalloc scatter");
+    }
+    int host[2] = {0, 0};
+    if (n) CK(nullptr, cudaMemcpyAsync(&host[0], start + nb, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(nullptr, cudaMemcpyAsync(&host[1], err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(nullptr, cudaStreamSynchronize(s));
+    *kept = (unsigned)host[0];
+    return host[1];
+}

@@ -45,6 +45,7 @@ extern "C" {
 #define MPM_ERR_CONFIG_KEY   106  /* required key "InputRawPoints" missing   */
 #define MPM_ERR_SORT_RANGE   107  /* a particle's cell key lies outside grid */
 #define MPM_ERR_STATE        108  /* call out of order (e.g. step before upload) */
+#define MPM_ERR_NOALLOC_LIMIT 109 /* size beyond the fixed scratch of mpm_sort_permutation_noalloc */
 
 #define MPM_PRECISION_FP64   0    /* FP64 state and transfers; 3x3 SVD in FP32
                                      exactly as the reference (helper_math.cuh) */
@@ -169,6 +170,28 @@ int  mpm_synchronize(mpm_handle* h);
 int  mpm_get_params(mpm_handle* h, SimParams3D* out);
 /* Number of particles currently held (after sorts that drop disabled ones). */
 int  mpm_count(mpm_handle* h, unsigned* n);
+/* No counterpart in the reference. The stable cell-key sort of mpm_sort
+ * (same keys, same permutation) for callers that must not have the library
+ * allocate device memory: programs that plan and own every byte of the GPU
+ * (their own pool or a fixed footprint), and loops that cannot take the
+ * latency and device-wide synchronisation of a cudaMalloc mid-run. The
+ * caller passes device pointers: soa (28 rows of `pitch` doubles, the
+ * HostSideSOA row layout, n particles) and perm (n unsigned); perm receives
+ * the source index of each kept particle in sorted order and *kept (host)
+ * their count, disabled particles dropped. The call allocates nothing: its
+ * scratch is a fixed array of about 10 MB compiled into the library, held by
+ * every GPU that loads it until the process exits, which limits a call to
+ * n <= 524,288 particles and (GridXTotal + 2*GridHaloSize + 1)*GridY*GridZ + 1
+ * <= 1,048,576 cell keys (MPM_ERR_NOALLOC_LIMIT beyond). The first call on a
+ * device looks up that array's device address there (with the device
+ * current); make that first call before any stream capture. Work is issued
+ * on `stream` (a cudaStream_t, NULL = legacy default) on the current device,
+ * and the call waits for it. All calls share the one array: calls that
+ * overlap on the GPU (other host threads, other streams) race and must be
+ * serialised by the caller. Returns 0, 107 if a key falls outside the grid,
+ * or an error code. */
+int  mpm_sort_permutation_noalloc(const SimParams3D* prms, const double* soa, unsigned pitch,
+                                  unsigned n, unsigned* perm, unsigned* kept, void* stream);
 /* Text of the last CUDA failure seen by this thread (MPM_ERR_CUDA). */
 const char* mpm_last_error_string(void);
 
