@@ -353,6 +353,120 @@ __device__ __forceinline__ bool p2g_scatter_tile(const DevParams& P, float4* __r
     return true;
 }
 
+// Shared-memory tile in 32-bit block fixed point. As p2g_scatter_tile, but
+// the tile holds integers: each contribution v is added as round(v * 2^e)
+// with native 32-bit shared atomics (order-independent sums), e chosen per
+// block from its largest possible contribution so that a node can absorb up
+// to 128 of them without overflow (2^-23 of that bound per unit). The flush
+// converts each node back to FP32 and adds it to the grid with one float4
+// atomic. Must be called by the whole block of 128 threads.
+__device__ __forceinline__ int fx32_exponent(float bound) {
+    int ex;
+    frexpf(fmaxf(bound, 1e-30f), &ex);   // bound < 2^ex
+    return 23 - ex;                        // 128 * bound * 2^e < 2^30
+}
+
+template <int BLOCK>
+__device__ __forceinline__ bool p2g_scatter_tile_fx(const DevParams& P, float4* __restrict__ acc, int* __restrict__ tile,
+                                                    int tile_cap, bool active, bool inside, const int base[3],
+                                                    const float fx[3], float mass, const float mv[3],
+                                                    const float S[3][3], int lane) {
+    __shared__ int s_box[8];
+    if (threadIdx.x < 3) { s_box[threadIdx.x] = INT_MAX; s_box[3 + threadIdx.x] = INT_MIN; }
+    if (threadIdx.x == 0) { s_box[6] = 0; s_box[7] = 0; }
+    __syncthreads();
+    const bool in_box = active && inside;
+    // bound of |w (m v + S (x_i - x_p))| over the stencil: w <= 1, |x_i - x_p| <= 1.5 h per axis
+    const float h15 = 1.5f * (float)P.h;
+    float pb = 0.f;
+    if (in_box) {
+#pragma unroll
+        for (int m = 0; m < 3; m++)
+            pb = fmaxf(pb, fabsf(mv[m]) + h15 * (fabsf(S[m][0]) + fabsf(S[m][1]) + fabsf(S[m][2])));
+    }
+    float mb = in_box ? mass : 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        int lo = in_box ? base[d] : INT_MAX, hi = in_box ? base[d] + 2 : INT_MIN;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if (lane == 0) { atomicMin(&s_box[d], lo); atomicMax(&s_box[3 + d], hi); }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        pb = fmaxf(pb, __shfl_xor_sync(0xffffffffu, pb, o));
+        mb = fmaxf(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+    }
+    if (lane == 0) { atomicMax(&s_box[6], __float_as_int(pb)); atomicMax(&s_box[7], __float_as_int(mb)); }
+    __syncthreads();
+    const int bx = s_box[0], by = s_box[1], bz = s_box[2];
+    if (bx > s_box[3]) return true;   // no particle of the block is inside
+    const int ex = s_box[3] - bx + 1, ey = s_box[4] - by + 1, ez = s_box[5] - bz + 1;
+    const long long vol = (long long)ex * ey * ez;
+    if (vol > tile_cap) return false;
+    const int nv = (int)vol;
+    const int e_p = fx32_exponent(__int_as_float(s_box[6]));
+    const int e_m = fx32_exponent(__int_as_float(s_box[7]));
+    const float sc_p = ldexpf(1.0f, e_p), sc_m = ldexpf(1.0f, e_m);
+    for (int k = threadIdx.x; k < 4 * nv; k += BLOCK) tile[k] = 0;
+    __syncthreads();
+    if (active && !inside) {
+        p2g_scatter_mixed<false>(P, acc, active, inside, base, fx, mass, mv, S, lane);
+    } else if (in_box) {
+        const int t0 = ((base[0] - bx) * ey + (base[1] - by)) * ez + (base[2] - bz);
+        float ww[3][3];
+        quad_weights<float>(fx, ww);
+        const float h = (float)P.h;
+        const float msc = mass * sc_m;
+        float Ssc[3][3], mvsc[3];
+#pragma unroll
+        for (int m = 0; m < 3; m++) {
+            mvsc[m] = mv[m] * sc_p;
+#pragma unroll
+            for (int k = 0; k < 3; k++) Ssc[m][k] = S[m][k] * sc_p;
+        }
+#pragma unroll 1
+        for (int a = 0; a < 3; a++) {
+            const float dx = (a - fx[0]) * h;
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                const float dy = (b - fx[1]) * h;
+                const float wab = ww[a][0] * ww[b][1];
+                const int tb = t0 + (a * ey + b) * ez;
+                float part[3];
+#pragma unroll
+                for (int m = 0; m < 3; m++) part[m] = mvsc[m] + Ssc[m][0] * dx + Ssc[m][1] * dy;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const float dz = (c - fx[2]) * h;
+                    const float W = wab * ww[c][2];
+                    const int t = tb + c;
+                    atomicAdd(tile + t, __float2int_rn(W * msc));
+                    atomicAdd(tile + nv + t, __float2int_rn(W * (part[0] + Ssc[0][2] * dz)));
+                    atomicAdd(tile + 2 * nv + t, __float2int_rn(W * (part[1] + Ssc[1][2] * dz)));
+                    atomicAdd(tile + 3 * nv + t, __float2int_rn(W * (part[2] + Ssc[2][2] * dz)));
+                }
+            }
+        }
+    }
+    __syncthreads();
+    const float inv_m = ldexpf(1.0f, -e_m), inv_p = ldexpf(1.0f, -e_p);
+    const int slab = (int)P.slab, gz = P.Gz;
+    const int g0 = ((bx + P.halo) * P.Gy + by) * gz + bz;
+    for (int t = threadIdx.x; t < nv; t += BLOCK) {
+        const int m = tile[t];
+        if (m == 0) continue;
+        const int tz = t % ez, ty = (t / ez) % ey, tx = t / (ez * ey);
+        atomicAdd(acc + (g0 + tx * slab + ty * gz + tz),
+                  make_float4((float)m * inv_m, (float)tile[nv + t] * inv_p, (float)tile[2 * nv + t] * inv_p,
+                              (float)tile[3 * nv + t] * inv_p));
+    }
+    return true;
+}
+
 // P2G payload of a particle: S = m C - dt V Dp^-1 tau (mpm_kernels.cuh:63)
 __device__ __forceinline__ void p2g_payload_mixed(const DevParams& P, const float E[3][3], const float C[3][3],
                                                   const float v[3], bool liquid, float Jp, float& mass, float mv[3],
@@ -426,7 +540,8 @@ __global__ void __launch_bounds__(256) k_p2g_mixed(DevParams P, MixedState s, in
 
 // Fused G2P (this step) -> P2G (next step). do_p2g = 0 gives a plain G2P.
 // SCATTER: 0 = warp-reduced direct float4 atomics, 1 = direct float4
-// atomics, 2 = shared-memory tile (falls back to 0 when the box is too big)
+// atomics, 2 = FP32 shared-memory tile, 3 = int32 fixed-point shared-memory
+// tile (2 and 3 fall back to 0 when the box is too big)
 template <int MINB, int SCATTER>
 __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedState s, int n,
                                                            const float4* __restrict__ vel, float4* __restrict__ acc,
@@ -546,6 +661,9 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
             for (int c = 0; c < 3; c++) S[r][c] = 0.f;
     }
     if (SCATTER == 2 && p2g_scatter_tile<128>(P, acc, mixed_tile, tile_cap, active, inside, base, fx, mass, mv, S, lane))
+        return;
+    if (SCATTER == 3 && p2g_scatter_tile_fx<128>(P, acc, reinterpret_cast<int*>(mixed_tile), tile_cap, active, inside,
+                                                 base, fx, mass, mv, S, lane))
         return;
     if (SCATTER == 1) p2g_scatter_mixed<false>(P, acc, active, inside, base, fx, mass, mv, S, lane);
     else p2g_scatter_mixed<true>(P, acc, active, inside, base, fx, mass, mv, S, lane);

@@ -284,12 +284,13 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq) {
     const int n = (int)h->n;
     if (n == 0) return MPM_OK;
     const unsigned nb = blocks_for(n, 128);
-    const size_t tsm = h->mixed_scatter == 2 ? sizeof(float) * 4 * kMixedTileNodes : 0;
+    const size_t tsm = h->mixed_scatter >= 2 ? sizeof(float) * 4 * kMixedTileNodes : 0;
 #define FUSED(MINB, SC)                                                                                          \
     k_g2p2g_mixed<MINB, SC><<<nb, 128, tsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,     \
                                                          record_pq, h->err, kMixedTileNodes)
 #define FUSED_SC(MINB)                              \
-    if (h->mixed_scatter == 2) FUSED(MINB, 2);      \
+    if (h->mixed_scatter == 3) FUSED(MINB, 3);      \
+    else if (h->mixed_scatter == 2) FUSED(MINB, 2); \
     else if (h->mixed_scatter == 1) FUSED(MINB, 1); \
     else FUSED(MINB, 0);
     if (h->mixed_variant == 1) { FUSED_SC(5) }
@@ -927,7 +928,7 @@ int mpm_testing_download_grid(mpm_handle* h, double* out, int which) {
 }
 
 int mpm_testing_set_p2g_variant(mpm_handle* h, int variant) {
-    if (!h || variant < 0 || variant > 7) return MPM_ERR_ARG;
+    if (!h || variant < 0 || variant > 8) return MPM_ERR_ARG;
     if (variant >= 5) {
         h->mixed_scatter = variant - 5;
         return MPM_OK;

@@ -17,8 +17,9 @@ extern "C" {
  * global atomics, 2 = as 1 with a warp reduction over particles sharing a
  * base cell, 3 = as 0 with that warp reduction, 4 = shared-memory tile in
  * 64-bit block fixed point over 1024-particle chunks. In the mixed mode,
- * 5/6/7 select the fused kernel's scatter: 5 = warp-reduced float4 atomics,
- * 6 = float4 atomics per particle (default), 7 = FP32 shared-memory tile. */
+ * 5..8 select the fused kernel's scatter: 5 = warp-reduced float4 atomics,
+ * 6 = float4 atomics per particle (default), 7 = FP32 shared-memory tile,
+ * 8 = int32 block fixed-point shared-memory tile. */
 int mpm_testing_set_p2g_variant(mpm_handle* h, int variant);
 
 /* G2P kernel occupancy target (FP64 modes): 0 = 4 blocks of 128 threads per

@@ -34,7 +34,7 @@ def test_upload_download_round_trip():
     assert np.array_equal(util_bits(out), util_bits(soa))
 
 
-@pytest.mark.parametrize("scatter", [5, 6, 7])
+@pytest.mark.parametrize("scatter", [5, 6, 7, 8])
 def test_single_step_phases_close_to_oracle(scatter):
     prms, soa = perturbed_block(n=4000, seed=31)
     n = soa.shape[1]
@@ -73,7 +73,7 @@ def test_single_step_phases_close_to_oracle(scatter):
     assert rel_dev(out[IDX_JP_INV][same], ref[IDX_JP_INV][same]) < 1e-5
 
 
-@pytest.mark.parametrize("scatter", [5, 6, 7])
+@pytest.mark.parametrize("scatter", [5, 6, 7, 8])
 def test_force_history_within_1e3_of_fp64(scatter):
     prms, soa = perturbed_block(n=3000, seed=41, ind_velocity=0.5, crushed_frac=0.05, strong_frac=0.0)
     n = soa.shape[1]
