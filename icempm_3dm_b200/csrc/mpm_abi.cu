@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -21,6 +22,7 @@
 #include "device_common.cuh"
 #include "kernels_f64.cuh"
 #include "kernels_mixed.cuh"
+#include "adjoint_f64.cuh"
 #include "sort.cuh"
 
 using namespace icempm;
@@ -80,6 +82,18 @@ struct mpm_handle {
     bool p2g_ready = false;           // gacc holds the P2G of the current state
     int mixed_variant = 2;            // fused kernel occupancy target (test hook)
     int mixed_scatter = 1;            // fused kernel scatter: 0 warp-reduced, 1 direct (default), 2 tile (test hook)
+
+    // adjoint (FP64 modes): checkpoints of the recorded forward run
+    std::vector<double*> ckpt;        // particle state at substeps 0, k, 2k, ...
+    std::vector<SimParams3D> ckpt_prms;
+    std::vector<double*> seg;         // states of one segment during the reverse sweep
+    double* adj_A = nullptr;          // ADJ_ROWS x pitch particle adjoints
+    double* adj_cgrad = nullptr;      // dL/dc per particle
+    double* adj_Egrad = nullptr;      // dL/dE
+    double* adj_g7 = nullptr;         // recomputed grid: m, P, final v (7 x gstride)
+    double* adj_gb7 = nullptr;        // grid adjoints: vb, mb, Pb (7 x gstride)
+    int adj_steps = 0, adj_every = 0;
+    bool adj_ready = false;
 
     int p2g_variant = 2;              // see mpm_testing_set_p2g_variant
     int g2p_variant = 2;              // see mpm_testing_set_g2p_variant
@@ -174,6 +188,11 @@ void free_all(mpm_handle* h) {
     cudaFree(h->s_bucket); cudaFree(h->s_count); cudaFree(h->s_start); cudaFree(h->s_perm);
     cudaFree(h->chunk_bound);
     cudaFree(h->mx); cudaFree(h->p0f); cudaFree(h->gacc); cudaFree(h->gvel);
+    for (double* c : h->ckpt) cudaFree(c);
+    for (double* c : h->seg) cudaFree(c);
+    h->ckpt.clear();
+    h->seg.clear();
+    cudaFree(h->adj_A); cudaFree(h->adj_cgrad); cudaFree(h->adj_Egrad); cudaFree(h->adj_g7); cudaFree(h->adj_gb7);
     for (int* p : h->scan_levels) cudaFree(p);
     h->scan_levels.clear();
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -249,6 +268,11 @@ int launch_p2g(mpm_handle* h) {
             if (chunks > h->chunk_bound_cap) {
                 cudaFree(h->chunk_bound);
     cudaFree(h->mx); cudaFree(h->p0f); cudaFree(h->gacc); cudaFree(h->gvel);
+    for (double* c : h->ckpt) cudaFree(c);
+    for (double* c : h->seg) cudaFree(c);
+    h->ckpt.clear();
+    h->seg.clear();
+    cudaFree(h->adj_A); cudaFree(h->adj_cgrad); cudaFree(h->adj_Egrad); cudaFree(h->adj_g7); cudaFree(h->adj_gb7);
                 h->chunk_bound = nullptr;
                 CK(h, cudaMalloc(&h->chunk_bound, sizeof(float) * chunks));
                 CK(h, cudaMemsetAsync(h->chunk_bound, 0, sizeof(float) * chunks, h->stream));
@@ -1037,4 +1061,166 @@ extern "C" int mpm_sort_permutation_noalloc(const SimParams3D* prms, const doubl
     CK(nullptr, cudaStreamSynchronize(s));
     *kept = (unsigned)host[0];
     return host[1];
+}
+
+// ------------------------------------------------------------------ adjoint
+
+namespace {
+
+size_t state_bytes(const mpm_handle* h) { return sizeof(double) * MPM_N_PTS_ARRAYS * h->pitch; }
+
+// One FP64 substep of Model3D::Step on the particle rows at h->pts.
+int fp64_substep(mpm_handle* h, double* force3) {
+    SimParams3D& p = h->prms;
+    p.SimulationTime += p.InitialTimeStep;
+    p.indenter_x = p.indenter_x_initial + p.SimulationTime * p.IndVelocity;
+    int r;
+    if ((r = reset_grid(h))) return r;
+    if ((r = launch_p2g(h))) return r;
+    if ((r = launch_update(h, p.indenter_x, p.indenter_y, force3))) return r;
+    const int record = (p.SimulationStep % p.UpdateEveryNthStep) == 0;
+    if ((r = launch_g2p(h, record))) return r;
+    p.SimulationStep += 1;
+    return MPM_OK;
+}
+
+int ensure_adjoint_buffers(mpm_handle* h, int nsteps, int every) {
+    const int nck = (nsteps + every - 1) / every;
+    while ((int)h->ckpt.size() < nck) {
+        double* b = nullptr;
+        CK(h, cudaMalloc(&b, state_bytes(h)));
+        h->ckpt.push_back(b);
+    }
+    while ((int)h->seg.size() < every + 1) {
+        double* b = nullptr;
+        CK(h, cudaMalloc(&b, state_bytes(h)));
+        h->seg.push_back(b);
+    }
+    h->ckpt_prms.resize(nck);
+    if (!h->adj_A) {
+        CK(h, cudaMalloc(&h->adj_A, sizeof(double) * ADJ_ROWS * h->pitch));
+        CK(h, cudaMalloc(&h->adj_cgrad, sizeof(double) * h->pitch));
+        CK(h, cudaMalloc(&h->adj_Egrad, sizeof(double)));
+        CK(h, cudaMalloc(&h->adj_g7, sizeof(double) * 7 * (size_t)h->dp.gstride));
+        CK(h, cudaMalloc(&h->adj_gb7, sizeof(double) * 7 * (size_t)h->dp.gstride));
+    }
+    return MPM_OK;
+}
+
+AdjParams adj_params(const mpm_handle* h) {
+    const SimParams3D& p = h->prms;
+    AdjParams q;
+    q.rc.pmax = p.IceCompressiveStrength;
+    q.rc.tensile = p.IceTensileStrength;
+    q.rc.shear = p.IceShearStrength;
+    q.rc.tan_phi = p.DP_tan_phi;
+    const double nu = p.PoissonsRatio;
+    q.dmu_dE = 1.0 / (2 * (1 + nu));
+    q.dkappa_dE = 2.0 / 3.0 * q.dmu_dE + nu / ((1 + nu) * (1 - 2 * nu));
+    q.s4 = 4.0 / (p.cellsize * p.cellsize);
+    return q;
+}
+
+}  // namespace
+
+extern "C" int mpm_adjoint_forward(mpm_handle* h, int nsteps, int ckpt_every, double* force_hist) {
+    if (!h || nsteps <= 0 || ckpt_every <= 0) return MPM_ERR_ARG;
+    if (!h->uploaded) return MPM_ERR_STATE;
+    if (is_mixed(h)) return MPM_ERR_ARG;   // the adjoint differentiates the FP64 step
+    int r = ensure_adjoint_buffers(h, nsteps, ckpt_every);
+    if (r) return r;
+    if (nsteps > h->force_steps_cap) {
+        CK(h, cudaStreamSynchronize(h->stream));
+        cudaFree(h->force_steps);
+        h->force_steps = nullptr;
+        CK(h, cudaMalloc(&h->force_steps, sizeof(double) * 3 * (size_t)nsteps));
+        h->force_steps_cap = nsteps;
+    }
+    CK(h, cudaMemsetAsync(h->force_steps, 0, sizeof(double) * 3 * (size_t)nsteps, h->stream));
+    for (int s = 0; s < nsteps; s++) {
+        if (s % ckpt_every == 0) {
+            CK(h, cudaMemcpyAsync(h->ckpt[s / ckpt_every], h->pts, state_bytes(h), cudaMemcpyDeviceToDevice, h->stream));
+            h->ckpt_prms[s / ckpt_every] = h->prms;
+        }
+        if ((r = fp64_substep(h, h->force_steps + 3 * s))) return r;
+    }
+    if (force_hist)
+        CK(h, cudaMemcpyAsync(force_hist, h->force_steps, sizeof(double) * 3 * (size_t)nsteps, cudaMemcpyDeviceToHost,
+                              h->stream));
+    h->adj_steps = nsteps;
+    h->adj_every = ckpt_every;
+    h->adj_ready = true;
+    int code = 0;
+    r = read_error(h, &code);
+    return r ? r : code;
+}
+
+extern "C" int mpm_adjoint_backward(mpm_handle* h, const double* dL_dforce, double* dL_dcohesion, double* dL_dE) {
+    if (!h || !dL_dforce) return MPM_ERR_ARG;
+    if (!h->adj_ready) return MPM_ERR_STATE;
+    const int N = h->adj_steps, k = h->adj_every, n = (int)h->n;
+    const DevParams dp = h->dp;
+    const AdjParams q = adj_params(h);
+    const size_t gs = (size_t)dp.gstride;
+    CK(h, cudaMemsetAsync(h->adj_A, 0, sizeof(double) * ADJ_ROWS * h->pitch, h->stream));
+    CK(h, cudaMemsetAsync(h->adj_cgrad, 0, sizeof(double) * h->pitch, h->stream));
+    CK(h, cudaMemsetAsync(h->adj_Egrad, 0, sizeof(double), h->stream));
+    double* const pts_final = h->pts;
+    const SimParams3D prms_final = h->prms;
+    int r = MPM_OK;
+    const int nseg = (N + k - 1) / k;
+    for (int j = nseg - 1; j >= 0 && !r; j--) {
+        const int s0 = j * k, s1 = std::min(N, s0 + k);
+        // recompute the segment's states from its checkpoint
+        std::vector<SimParams3D> sp(s1 - s0);
+        CK(h, cudaMemcpyAsync(h->seg[0], h->ckpt[j], state_bytes(h), cudaMemcpyDeviceToDevice, h->stream));
+        h->prms = h->ckpt_prms[j];
+        for (int s = s0; s < s1 && !r; s++) {
+            double* next = h->seg[s - s0 + 1];
+            CK(h, cudaMemcpyAsync(next, h->seg[s - s0], state_bytes(h), cudaMemcpyDeviceToDevice, h->stream));
+            h->pts = next;
+            r = fp64_substep(h, h->force_phase);
+            sp[s - s0] = h->prms;   // holds this substep's indenter position
+        }
+        h->pts = pts_final;
+        if (r) break;
+        // reverse the segment
+        for (int s = s1 - 1; s >= s0; s--) {
+            const double* Sn = h->seg[s - s0];
+            const double* Sn1 = h->seg[s - s0 + 1];
+            const double ix = sp[s - s0].indenter_x, iy = sp[s - s0].indenter_y;
+            CK(h, cudaMemsetAsync(h->adj_g7, 0, sizeof(double) * 4 * gs, h->stream));
+            k_p2g_warpagg_f64<<<blocks_for(n, 256), 256, 0, h->stream>>>(dp, Sn, h->pitch, n, h->adj_g7, h->err);
+            k_adj_update_record<256><<<blocks_for(dp.nodes, 256), 256, 0, h->stream>>>(dp, h->adj_g7, ix, iy);
+            CK(h, cudaMemsetAsync(h->adj_gb7, 0, sizeof(double) * 7 * gs, h->stream));
+            k_adj_g2p_rev<128><<<blocks_for(n, 128), 128, 0, h->stream>>>(dp, q, Sn, Sn1, h->pitch, n, h->adj_g7, h->p0,
+                                                                         h->adj_A, h->adj_gb7, h->adj_cgrad,
+                                                                         h->adj_Egrad);
+            k_adj_node_rev<256><<<blocks_for(dp.nodes, 256), 256, 0, h->stream>>>(
+                dp, h->adj_g7, h->adj_gb7, ix, iy, dL_dforce[3 * s], dL_dforce[3 * s + 1], dL_dforce[3 * s + 2]);
+            k_adj_p2g_rev<128><<<blocks_for(n, 128), 128, 0, h->stream>>>(dp, q, Sn, h->pitch, n, h->adj_gb7, h->adj_A,
+                                                                         h->adj_Egrad);
+            CK_LAUNCH(h, "adjoint kernels");
+        }
+    }
+    h->pts = pts_final;
+    h->prms = prms_final;
+    if (r) return r;
+    if (dL_dcohesion && n)
+        CK(h, cudaMemcpyAsync(dL_dcohesion, h->adj_cgrad, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    double eg = 0;
+    CK(h, cudaMemcpyAsync(&eg, h->adj_Egrad, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (dL_dE) *dL_dE = eg;
+    return MPM_OK;
+}
+
+extern "C" int mpm_adjoint_state(mpm_handle* h, double* adj, unsigned pitch) {
+    if (!h || !adj || pitch < h->n) return MPM_ERR_ARG;
+    if (!h->adj_ready || !h->adj_A) return MPM_ERR_STATE;
+    if (h->n)
+        CK(h, cudaMemcpy2DAsync(adj, sizeof(double) * pitch, h->adj_A, sizeof(double) * h->pitch, sizeof(double) * h->n,
+                                ADJ_ROWS, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
 }

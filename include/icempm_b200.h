@@ -170,6 +170,26 @@ int  mpm_synchronize(mpm_handle* h);
 int  mpm_get_params(mpm_handle* h, SimParams3D* out);
 /* Number of particles currently held (after sorts that drop disabled ones). */
 int  mpm_count(mpm_handle* h, unsigned* n);
+/* ---------------------------------------------------------------- adjoint
+ * No counterpart in the reference (new, for calibrating ice strength).
+ * Reverse-mode gradients of a loss on the indenter force history with
+ * respect to per-particle cohesion and Young's modulus, through the FP64 step
+ * (FP64 precision modes; MPM_ERR_ARG on a mixed handle). */
+
+/* Runs nsteps substeps exactly as mpm_step (no sorting) from the current
+ * state, saving the particle state every ckpt_every substeps on the device;
+ * force_hist (may be NULL) receives nsteps x 3 forces. The state advances. */
+int  mpm_adjoint_forward(mpm_handle* h, int nsteps, int ckpt_every, double* force_hist);
+/* Reverse sweep of the last mpm_adjoint_forward: each segment is recomputed
+ * from its checkpoint, then reversed substep by substep. dL_dforce: nsteps x 3
+ * (dL/d force of each substep). dL_dcohesion (n doubles, may be NULL) and
+ * *dL_dE (may be NULL) receive the gradients; the cohesion gradient is per
+ * particle in the handle's current order (mpm_download_ids maps it). */
+int  mpm_adjoint_backward(mpm_handle* h, const double* dL_dforce, double* dL_dcohesion, double* dL_dE);
+/* Adjoints of the initial particle state after mpm_adjoint_backward: 25 rows
+ * [x(3), v(3), C(9), F(9), Jp_inv] of row stride pitch >= n. */
+int  mpm_adjoint_state(mpm_handle* h, double* adj, unsigned pitch);
+
 /* No counterpart in the reference. The stable cell-key sort of mpm_sort
  * (same keys, same permutation) for callers that must not have the library
  * allocate device memory: programs that plan and own every byte of the GPU

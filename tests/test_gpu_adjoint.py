@@ -1,0 +1,111 @@
+"""Adjoint of the FP64 step (mpm_adjoint_forward / mpm_adjoint_backward)
+against central finite differences through the forward step, for the
+gradient of a linear functional of the indenter force history with respect
+to per-particle cohesion, Young's modulus and the initial particle state.
+
+Tolerance: 1e-3 relative (the north star's bound), on the entries whose
+gradient is not negligible. FP64 forward, FP64 SVD (the precision the
+adjoint differentiates).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from icempm_3dm_b200 import MPMHandle, PRECISION_FP64_SVD64
+from icempm_3dm_b200._lib import LIB, LIB as _L, POSX, VELX, check, dptr
+from icempm_3dm_b200._lib import SimParams3D
+from tests.helpers import perturbed_block
+
+pytestmark = pytest.mark.gpu
+
+
+def case(n=1500, seed=7):
+    prms, soa = perturbed_block(n=n, seed=seed, crushed_frac=0.4, strong_frac=0.15, ind_velocity=0.5,
+                                dims=(0.12, 0.08, 0.08))
+    rng = np.random.default_rng(seed)
+    cohesion = 3e5 * np.exp(0.3 * rng.standard_normal(soa.shape[1]))
+    return prms, soa, cohesion
+
+
+def loss(prms, soa, cohesion, wgt, nsteps):
+    with MPMHandle(prms, soa.shape[1], PRECISION_FP64_SVD64) as h:
+        h.upload(soa, cohesion=cohesion)
+        hist = h.step(nsteps)
+    return float(np.sum(wgt * hist))
+
+
+def adjoint(prms, soa, cohesion, wgt, nsteps, every):
+    n = soa.shape[1]
+    with MPMHandle(prms, n, PRECISION_FP64_SVD64) as h:
+        h.upload(soa, cohesion=cohesion)
+        hist = np.zeros((nsteps, 3))
+        check(LIB.mpm_adjoint_forward(h._h, nsteps, every, dptr(hist)), "adjoint forward")
+        dc = np.zeros(n)
+        dE = ctypes.c_double(0)
+        w = np.ascontiguousarray(wgt, dtype=np.float64)
+        check(LIB.mpm_adjoint_backward(h._h, dptr(w), dptr(dc), ctypes.byref(dE)), "adjoint backward")
+        adj = np.zeros((25, n))
+        check(LIB.mpm_adjoint_state(h._h, dptr(adj), n), "adjoint state")
+    return float(np.sum(wgt * hist)), dc, dE.value, adj
+
+
+def with_E(prms, E):
+    p = prms.copy()
+    p.YoungsModulus = E
+    LIB.mpm_params_compute_camclay(p)
+    LIB.mpm_params_compute_helper_variables(p)
+    return p
+
+
+@pytest.mark.parametrize("nsteps,every", [(1, 1), (8, 3)])
+def test_adjoint_matches_finite_differences(nsteps, every):
+    prms, soa, coh = case()
+    rng = np.random.default_rng(1)
+    wgt = rng.standard_normal((nsteps, 3))
+    wgt[:, 2] = 0.0
+    L0, dc, dE, adj = adjoint(prms, soa, coh, wgt, nsteps, every)
+    assert L0 != 0.0
+    assert L0 == pytest.approx(loss(prms, soa, coh, wgt, nsteps), rel=1e-9)
+    print(f"\nL = {L0:.6e}, nonzero dL/dc: {np.count_nonzero(dc)} of {dc.size}")
+    if nsteps == 1:
+        # the force of a substep is measured in the grid update, before the
+        # return map reads the cohesion: one substep does not depend on it
+        assert not np.any(dc)
+    else:
+        assert np.count_nonzero(dc) > dc.size // 2
+    report = []
+
+    # Young's modulus
+    eps = 1e-6
+    E = prms.YoungsModulus
+    fd = (loss(with_E(prms, E * (1 + eps)), soa, coh, wgt, nsteps) -
+          loss(with_E(prms, E * (1 - eps)), soa, coh, wgt, nsteps)) / (2 * eps * E)
+    report.append(("E", fd, dE))
+
+    # cohesion of the particles with the largest gradients
+    for i in np.argsort(-np.abs(dc))[:4]:
+        if abs(dc[i]) == 0:
+            continue
+        cp, cm = coh.copy(), coh.copy()
+        cp[i] *= 1 + 1e-4
+        cm[i] *= 1 - 1e-4
+        fd = (loss(prms, soa, cp, wgt, nsteps) - loss(prms, soa, cm, wgt, nsteps)) / (2e-4 * coh[i])
+        report.append((f"c[{i}]", fd, dc[i]))
+
+    # initial velocity and position of the particles with the largest velocity adjoints
+    for row, off, h in ((VELX, 3, 1e-5), (POSX, 0, 1e-7)):
+        g = adj[off:off + 3]
+        i = int(np.argmax(np.abs(g).max(axis=0)))
+        d = int(np.argmax(np.abs(g[:, i])))
+        sp, sm = soa.copy(), soa.copy()
+        sp[row + d, i] += h
+        sm[row + d, i] -= h
+        fd = (loss(prms, sp, coh, wgt, nsteps) - loss(prms, sm, coh, wgt, nsteps)) / (2 * h)
+        report.append((f"row{row + d}[{i}]", fd, g[d, i]))
+
+    print("\n".join(f"{name:>14s}  fd {fd: .9e}  adjoint {ad: .9e}" for name, fd, ad in report))
+    assert all(abs(ad) > 0 for _, _, ad in report), report          # non-trivial gradients
+    assert len(report) == (3 if nsteps == 1 else 7)
+    bad = [(name, fd, ad) for name, fd, ad in report if abs(fd - ad) > 1e-3 * max(abs(fd), abs(ad), 1e-30)]
+    assert not bad, report
