@@ -44,6 +44,10 @@ void or_svd3x3_f32(const double A[9], double U[9], double S[3], double V[9]);
 /* The same algorithm carried out in double with `sweeps` Jacobi sweeps (the
  * "FP64 SVD" variant used as the high-accuracy reference). */
 void or_svd3x3_f64(const double A[9], double U[9], double S[3], double V[9], int sweeps);
+/* Forward-mode derivative of or_svd3x3_f64 in FP64 dual numbers: the tangent
+ * (dU, dS, dV) of the factors along the direction dA. */
+void or_svd3x3_dual(const double A[9], const double dA[9], double U[9], double dU[9], double S[3],
+                    double dS[3], double V[9], double dV[9], int sweeps);
 
 /* Cell key of ProxyPoint3D::getCellIndex (proxypoint3d.cpp:158-163). */
 int or_cell_key(const SimParams3D* prms, double x, double y, double z);
@@ -78,6 +82,17 @@ int or_g2p(const SimParams3D* prms, double* soa, unsigned pitch, unsigned n,
  * grid: scratch of 4*or_grid_nodes doubles. force3: this substep's force. */
 int or_step(SimParams3D* prms, double* soa, unsigned pitch, unsigned n, double* grid,
             double* sensor, double force3[3], const double* p0, int svd_mode, int nthreads);
+
+/* FP64 dual-number forward-mode derivative of nsteps substeps of or_step
+ * (serial, FP64 SVD): soa/dsoa are the initial state and its tangent (rows
+ * and pitch as for soa), p0/dp0 (may be NULL) the per-particle apex shift
+ * and its tangent, dE the tangent of YoungsModulus (carried into mu and
+ * kappa). On return soa/dsoa hold the final state and its tangent and
+ * force_hist/dforce_hist[3*nsteps] the indenter force of every substep and
+ * its tangent. prms advances like or_step. Returns 0 or 70..75. */
+int or_dual_steps(SimParams3D* prms, double* soa, double* dsoa, unsigned pitch, unsigned n,
+                  const double* p0, const double* dp0, double dE, int nsteps,
+                  double* force_hist, double* dforce_hist);
 
 #ifdef __cplusplus
 }

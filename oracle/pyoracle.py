@@ -41,6 +41,10 @@ def _load():
     lib.or_step.restype = ctypes.c_int
     lib.or_step.argtypes = [ctypes.c_void_p, _dp, ctypes.c_uint, ctypes.c_uint, _dp, _dp, _dp, _dp,
                             ctypes.c_int, ctypes.c_int]
+    lib.or_svd3x3_dual.argtypes = [_dp] * 8 + [ctypes.c_int]
+    lib.or_dual_steps.restype = ctypes.c_int
+    lib.or_dual_steps.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_uint, ctypes.c_uint, _dp, _dp,
+                                  ctypes.c_double, ctypes.c_int, _dp, _dp]
     return lib
 
 
@@ -66,6 +70,42 @@ def svd(a, mode="f32", sweeps=8):
     else:
         LIB.or_svd3x3_f64(_ptr(a), _ptr(u), _ptr(s), _ptr(v), sweeps)
     return u.reshape(3, 3), s, v.reshape(3, 3)
+
+
+def svd_dual(a, da, sweeps=8):
+    """Forward-mode derivative of the FP64 SVD along da: ((U, S, V), (dU, dS, dV))."""
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(9)
+    da = np.ascontiguousarray(da, dtype=np.float64).reshape(9)
+    out = [np.zeros(9), np.zeros(9), np.zeros(3), np.zeros(3), np.zeros(9), np.zeros(9)]
+    LIB.or_svd3x3_dual(_ptr(a), _ptr(da), *[_ptr(o) for o in out], sweeps)
+    u, du, s, ds, v, dv = out
+    return (u.reshape(3, 3), s, v.reshape(3, 3)), (du.reshape(3, 3), ds, dv.reshape(3, 3))
+
+
+def dual_steps(prms, soa, nsteps, dsoa=None, p0=None, dp0=None, dE=0.0):
+    """FP64 dual-number forward-mode derivative of nsteps substeps (FP64 SVD).
+
+    Returns (force_hist, dforce_hist, soa_final, dsoa_final); the tangents are
+    the directional derivatives along (dsoa, dp0, dE). prms is not modified.
+    """
+    import copy
+    P = copy.copy(prms)
+    s = np.array(soa, dtype=np.float64, copy=True, order="C")
+    ds = np.zeros_like(s) if dsoa is None else np.array(dsoa, dtype=np.float64, copy=True, order="C")
+    n = s.shape[1]
+    hist = np.zeros((nsteps, 3))
+    dhist = np.zeros((nsteps, 3))
+    p0p = None
+    if p0 is not None:
+        p0 = np.ascontiguousarray(p0, dtype=np.float64)
+        p0p = _ptr(p0)
+    if dp0 is not None:
+        dp0 = np.ascontiguousarray(dp0, dtype=np.float64)
+    err = LIB.or_dual_steps(ctypes.byref(P), _ptr(s), _ptr(ds), n, n, p0p,
+                            _ptr(dp0) if dp0 is not None else None, dE, nsteps, _ptr(hist), _ptr(dhist))
+    if err:
+        raise RuntimeError(f"oracle dual step error {err}")
+    return hist, dhist, s, ds
 
 
 def ref_svd(a):

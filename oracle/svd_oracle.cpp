@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include "dual.h"
 #include "mpm_oracle.h"
 
 namespace {
@@ -31,6 +32,10 @@ namespace {
 // in 64-bit extended precision and rounded once to float.
 inline float rsqrt_rn(float x) { return (float)(1.0L / sqrtl((long double)x)); }
 inline double rsqrt_rn(double x) { return 1.0 / std::sqrt(x); }
+inline Dual rsqrt_rn(const Dual& x) {
+    double r = 1.0 / std::sqrt(x.v);
+    return Dual(r, -0.5 * r * r * r * x.d);
+}
 
 template <typename T> struct SvdConst;
 template <> struct SvdConst<float> {
@@ -49,6 +54,14 @@ template <> struct SvdConst<double> {
     static double four_gamma_sq() { return 3.0 + 2.0 * std::sqrt(2.0); }
     static double sin_pi8() { return std::sin(MPM_PI / 8.0); }
     static double cos_pi8() { return std::cos(MPM_PI / 8.0); }
+};
+// Forward-mode derivative of the double variant: the constants carry no tangent.
+template <> struct SvdConst<Dual> {
+    static Dual tiny() { return SvdConst<double>::tiny(); }
+    static Dual small() { return SvdConst<double>::small(); }
+    static Dual four_gamma_sq() { return SvdConst<double>::four_gamma_sq(); }
+    static Dual sin_pi8() { return SvdConst<double>::sin_pi8(); }
+    static Dual cos_pi8() { return SvdConst<double>::cos_pi8(); }
 };
 
 // Symmetric 3x3 stored as s[i][j] (both halves kept in sync by writing the
@@ -151,8 +164,8 @@ void qr_givens(T B[3][3], T U[3][3], int i, int j, int col) {
     T a = B[i][col];            // pivot entry (row i)
     T b = B[j][col];                                            // entry to annihilate
     T sh = (b * b >= K::small()) ? b : (T)0;
-    T ch = std::fmax((T)0 - a, a);
-    ch = std::fmax(ch, K::small());
+    T ch = sc::fmax((T)0 - a, a);
+    ch = sc::fmax(ch, K::small());
     bool pos = a >= (T)0;
 
     T t2 = ch * ch;
@@ -318,4 +331,22 @@ extern "C" void or_svd3x3_f32(const double A[9], double U[9], double S[3], doubl
 
 extern "C" void or_svd3x3_f64(const double A[9], double U[9], double S[3], double V[9], int sweeps) {
     svd_entry<double>(A, U, S, V, sweeps);
+}
+
+// Forward-mode derivative of or_svd3x3_f64: the same iteration carried out in
+// dual numbers, A + eps dA -> (U, S, V) + eps (dU, dS, dV).
+extern "C" void or_svd3x3_dual(const double A[9], const double dA[9], double U[9], double dU[9], double S[3],
+                               double dS[3], double V[9], double dV[9], int sweeps) {
+    Dual a[3][3], u[3][3], s[3], v[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) a[i][j] = Dual(A[3 * i + j], dA[3 * i + j]);
+    svd_mcadams<Dual>(a, u, s, v, sweeps);
+    for (int i = 0; i < 3; i++) {
+        S[i] = s[i].v;
+        dS[i] = s[i].d;
+        for (int j = 0; j < 3; j++) {
+            U[3 * i + j] = u[i][j].v; dU[3 * i + j] = u[i][j].d;
+            V[3 * i + j] = v[i][j].v; dV[3 * i + j] = v[i][j].d;
+        }
+    }
 }

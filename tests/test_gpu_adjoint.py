@@ -1,11 +1,15 @@
 """Adjoint of the FP64 step (mpm_adjoint_forward / mpm_adjoint_backward)
-against central finite differences through the forward step, for the
-gradient of a linear functional of the indenter force history with respect
-to per-particle cohesion, Young's modulus and the initial particle state.
-
-Tolerance: 1e-3 relative (the north star's bound), on the entries whose
-gradient is not negligible. FP64 forward, FP64 SVD (the precision the
-adjoint differentiates).
+for the gradient of a linear functional of the indenter force history with
+respect to per-particle cohesion, Young's modulus and the initial particle
+state, checked two ways:
+  - against central finite differences through the GPU forward step, to
+    1e-3 relative (the required bound) on the largest gradient entries;
+  - against the oracle's FP64 dual-number forward mode (or_dual_steps, pinned
+    against finite differences in test_oracle_dual.py) along E, a random
+    cohesion direction and a random direction in the initial state, to 1e-6
+    relative (both are exact derivatives; they differ by FP64 rounding and the
+    summation order of the grid atomics).
+FP64 forward, FP64 SVD (the precision the adjoint differentiates).
 """
 import ctypes
 
@@ -13,8 +17,8 @@ import numpy as np
 import pytest
 
 from icempm_3dm_b200 import MPMHandle, PRECISION_FP64_SVD64
-from icempm_3dm_b200._lib import LIB, LIB as _L, POSX, VELX, check, dptr
-from icempm_3dm_b200._lib import SimParams3D
+from icempm_3dm_b200._lib import BP00, FE00, IDX_JP_INV, LIB, POSX, VELX, check, dptr
+from oracle import pyoracle as po
 from tests.helpers import perturbed_block
 
 pytestmark = pytest.mark.gpu
@@ -109,3 +113,42 @@ def test_adjoint_matches_finite_differences(nsteps, every):
     assert len(report) == (3 if nsteps == 1 else 7)
     bad = [(name, fd, ad) for name, fd, ad in report if abs(fd - ad) > 1e-3 * max(abs(fd), abs(ad), 1e-30)]
     assert not bad, report
+
+
+# rows of mpm_adjoint_state -> rows of the particle SoA
+ADJ_TO_SOA = ((0, POSX, 3), (3, VELX, 3), (6, BP00, 9), (15, FE00, 9), (24, IDX_JP_INV, 1))
+
+
+def test_adjoint_matches_dual_number_forward_mode():
+    nsteps, every = 8, 3
+    prms, soa, coh = case()
+    n = soa.shape[1]
+    rng = np.random.default_rng(2)
+    wgt = rng.standard_normal((nsteps, 3))
+    wgt[:, 2] = 0.0
+    L0, dc, dE, adj = adjoint(prms, soa, coh, wgt, nsteps, every)
+    p0 = coh / prms.DP_tan_phi
+    report = []
+
+    hist, dhist, _, _ = po.dual_steps(prms, soa, nsteps, p0=p0, dE=1.0)
+    assert float(np.sum(wgt * hist)) == pytest.approx(L0, rel=1e-7)
+    report.append(("E", float(np.sum(wgt * dhist)), dE))
+
+    r = coh * rng.standard_normal(n)
+    _, dhist, _, _ = po.dual_steps(prms, soa, nsteps, p0=p0, dp0=r / prms.DP_tan_phi)
+    report.append(("cohesion", float(np.sum(wgt * dhist)), float(r @ dc)))
+
+    dsoa = np.zeros_like(soa)
+    scale = {POSX: 1e-3, VELX: 0.05, BP00: 5.0, FE00: 1e-3}
+    for row, rows in ((POSX, 3), (VELX, 3), (BP00, 9), (FE00, 9)):
+        dsoa[row:row + rows] = scale[row] * rng.standard_normal((rows, n))
+    tension = soa[IDX_JP_INV] < 0.999          # Jp_inv = 1 sits on the tension test's switch
+    dsoa[IDX_JP_INV, tension] = 1e-3 * rng.standard_normal(int(tension.sum()))
+    _, dhist, _, _ = po.dual_steps(prms, soa, nsteps, dsoa=dsoa, p0=p0)
+    vjp = sum(float(np.sum(adj[a:a + k] * dsoa[s:s + k])) for a, s, k in ADJ_TO_SOA)
+    report.append(("state", float(np.sum(wgt * dhist)), vjp))
+
+    print("\n" + "\n".join(f"{name:>9s}  dual {t: .12e}  adjoint {a: .12e}" for name, t, a in report))
+    for name, t, a in report:
+        assert t != 0.0, name
+        assert abs(t - a) <= 1e-6 * abs(t), (name, t, a)
