@@ -208,5 +208,19 @@ def small_block(n=4000, seed=5, dims=(0.2, 0.1, 0.1), h=0.01, dt=1e-5, ind_veloc
     return make_block(cfg)
 
 
-__all__ = ["BlockConfig", "CONFIGS", "make_block", "make_params", "small_block", "jittered_lattice",
-           "splitmix64", "uniform", "normal", "BP00"]
+def calibration_block(n=20_000, penetration_cells=3, ind_velocity=2.0, cohesion_sigma_log=0.3):
+    """A smaller copy of the calib500k block (same spacing) for strength
+    calibration, with the indenter started penetration_cells cells into the
+    block and driven at ind_velocity: at calib500k's own 0.2 m/s over 200
+    substeps the indenter travels 0.4 mm and no particle crushes, so the
+    force history does not depend on cohesion at all."""
+    cfg = dataclasses.replace(CONFIGS["calib500k"], ind_velocity=ind_velocity,
+                              cohesion_sigma_log=cohesion_sigma_log)
+    prms, soa, coh = make_block(cfg, n=n)
+    prms.indenter_x_initial += penetration_cells * prms.cellsize
+    prms.indenter_x = prms.indenter_x_initial
+    return prms, soa, coh
+
+
+__all__ = ["BlockConfig", "CONFIGS", "make_block", "make_params", "small_block", "calibration_block",
+           "jittered_lattice", "splitmix64", "uniform", "normal", "BP00"]

@@ -148,6 +148,30 @@ class MPMHandle:
     def set_p2g_variant(self, v):
         check(LIB.mpm_testing_set_p2g_variant(self._h, v), "mpm_testing_set_p2g_variant")
 
+    # -- adjoint (FP64 handles)
+    def adjoint_forward(self, nsteps, ckpt_every):
+        """nsteps substeps with a device checkpoint every ckpt_every; returns
+        the (nsteps, 3) indenter force history."""
+        hist = np.zeros((nsteps, 3))
+        check(LIB.mpm_adjoint_forward(self._h, nsteps, ckpt_every, dptr(hist)), "mpm_adjoint_forward")
+        return hist
+
+    def adjoint_backward(self, dL_dforce):
+        """Reverse sweep for dL/d(force history); returns (dL/dcohesion per
+        particle in the handle's order, dL/dYoungsModulus)."""
+        g = np.ascontiguousarray(dL_dforce, dtype=np.float64).reshape(-1, 3)
+        dc = np.zeros(max(self.count(), 1))
+        dE = ctypes.c_double(0.0)
+        check(LIB.mpm_adjoint_backward(self._h, dptr(g), dptr(dc), ctypes.byref(dE)), "mpm_adjoint_backward")
+        return dc[:self.count()], dE.value
+
+    def adjoint_state(self):
+        """(25, n) adjoints of the initial state: x(3), v(3), C(9), F(9), Jp_inv."""
+        n = self.count()
+        adj = np.zeros((25, max(n, 1)))
+        check(LIB.mpm_adjoint_state(self._h, dptr(adj), adj.shape[1]), "mpm_adjoint_state")
+        return adj[:, :n]
+
 
 class GPU_Implementation6:
     """Method-for-method mirror of the reference class for one partition."""
