@@ -196,6 +196,89 @@ __device__ __forceinline__ void g2p_gather_mixed(const DevParams& P, const float
     }
 }
 
+// Gather with the warp's velocity box staged in shared memory. The warp's
+// lanes with an in-grid stencil (part) span a box of base cells; the box's
+// nodes (base .. base+2 per axis) are read from the grid once, row by row
+// along z (coalesced), into this warp's slice vbox[VCAP], and each lane then
+// gathers its 27 nodes from shared memory. A box larger than VCAP, or lanes
+// whose stencil leaves the grid, take the global gather. Called by the whole
+// warp (the box, the loads and __syncwarp are warp-wide).
+template <int VCAP>
+__device__ __forceinline__ void g2p_gather_staged(const DevParams& P, const float4* __restrict__ vel,
+                                                  float4* __restrict__ vbox, bool part, bool active,
+                                                  const int base[3], const float fx[3], float v[3], float C[3][3],
+                                                  int lane) {
+    const int lo0 = __reduce_min_sync(0xffffffffu, part ? base[0] : INT_MAX);
+    const int lo1 = __reduce_min_sync(0xffffffffu, part ? base[1] : INT_MAX);
+    const int lo2 = __reduce_min_sync(0xffffffffu, part ? base[2] : INT_MAX);
+    const int hi0 = __reduce_max_sync(0xffffffffu, part ? base[0] : INT_MIN);
+    const int hi1 = __reduce_max_sync(0xffffffffu, part ? base[1] : INT_MIN);
+    const int hi2 = __reduce_max_sync(0xffffffffu, part ? base[2] : INT_MIN);
+    int ey = 0, ez = 0;
+    bool staged = false;
+    if (lo0 <= hi0) {
+        const int ex = hi0 - lo0 + 3;
+        ey = hi1 - lo1 + 3;
+        ez = hi2 - lo2 + 3;
+        staged = (long long)ex * ey * ez <= VCAP;
+        if (staged) {
+            const int vol = ex * ey * ez;
+            const int slab = (int)P.slab, gz = P.Gz;
+            const int g0 = ((lo0 + P.halo) * P.Gy + lo1) * gz + lo2;
+            const float inv_ez = 1.0f / (float)ez, inv_ey = 1.0f / (float)ey;
+            for (int k = lane; k < vol; k += 32) {
+                const int row = (int)(((float)k + 0.5f) * inv_ez);   // k / ez (k, ez <= VCAP)
+                const int tz = k - row * ez;
+                const int tx = (int)(((float)row + 0.5f) * inv_ey);
+                const int ty = row - tx * ey;
+                vbox[k] = __ldg(vel + (g0 + tx * slab + ty * gz + tz));
+            }
+            __syncwarp();
+        }
+    }
+    if (part && staged) {
+        float ww[3][3];
+        quad_weights<float>(fx, ww);
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            v[d] = 0.f;
+#pragma unroll
+            for (int k = 0; k < 3; k++) C[d][k] = 0.f;
+        }
+        const float s4 = 4.0f * (float)P.h_inv;
+        const int t0 = ((base[0] - lo0) * ey + (base[1] - lo1)) * ez + (base[2] - lo2);
+#pragma unroll 1
+        for (int a = 0; a < 3; a++) {
+            const float wa = ww[a][0];
+            const float dpa = a - fx[0];
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                const float wab = wa * ww[b][1];
+                const float dpb = b - fx[1];
+                const int tb = t0 + a * ey * ez + b * ez;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const float4 nd = vbox[tb + c];
+                    const float w = wab * ww[c][2];
+                    const float nv[3] = {nd.x, nd.y, nd.z};
+                    const float dp[3] = {dpa, dpb, c - fx[2]};
+                    const float sw = s4 * w;
+#pragma unroll
+                    for (int r = 0; r < 3; r++) {
+                        v[r] += w * nv[r];
+                        const float swv = sw * nv[r];
+#pragma unroll
+                        for (int k = 0; k < 3; k++) C[r][k] += swv * dp[k];
+                    }
+                }
+            }
+        }
+    } else if (active) {
+        g2p_gather_mixed(P, vel, base, fx, v, C, !part);
+    }
+    __syncwarp();
+}
+
 // Return map of a crushed point in FP64 (mpm_kernels.cuh:486-544). Out of
 // line (it is rare and register-hungry); arguments and result travel by
 // value so that nothing of the caller is forced into local memory.
@@ -268,6 +351,56 @@ __device__ __forceinline__ void p2g_scatter_mixed(const DevParams& P, float4* __
                     }
                 }
                 if (!active || lane != leader) continue;
+                if (!inside && !node_inside(P, base[0] + a, base[1] + b, base[2] + c)) continue;
+                atomicAdd(acc + (ib + c), make_float4(val[0], val[1], val[2], val[3]));
+            }
+        }
+    }
+}
+
+// Scatter with pairs of particles that share a base cell merged in
+// registers: in cell-sorted order they sit in neighbouring lanes, so one
+// shuffle round per node moves the odd-ranked partner's four values to the
+// even-ranked lane, which issues the single float4 atomic for both. A third
+// particle of a cell (rank 2) pairs with a fourth or adds alone. Halves the
+// atomic traffic to L2 at ppc ~2 for 8 shuffles and adds per node.
+__device__ __forceinline__ void p2g_scatter_pairs(const DevParams& P, float4* __restrict__ acc, bool active,
+                                                  bool inside, const int base[3], const float fx[3], float mass,
+                                                  const float mv[3], const float S[3][3], int lane) {
+    const int i0 = ((base[0] + P.halo) * P.Gy + base[1]) * P.Gz + base[2];
+    const int key = (active && inside) ? i0 : -1 - lane;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    const int next_key = __shfl_down_sync(0xffffffffu, key, 1);
+    const bool absorb = lane < 31 && next_key == key && (rank & 1) == 0;
+    const bool absorbed = __shfl_up_sync(0xffffffffu, (int)absorb, 1) != 0 && lane > 0;
+    float ww[3][3];
+    quad_weights<float>(fx, ww);
+    const float h = (float)P.h;
+    const int slab = (int)P.slab, gz = P.Gz;
+#pragma unroll 1
+    for (int a = 0; a < 3; a++) {
+        const float dx = (a - fx[0]) * h;
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            const float dy = (b - fx[1]) * h;
+            const float wab = ww[a][0] * ww[b][1];
+            const int ib = i0 + a * slab + b * gz;
+            float part[3];
+#pragma unroll
+            for (int m = 0; m < 3; m++) part[m] = mv[m] + S[m][0] * dx + S[m][1] * dy;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float dz = (c - fx[2]) * h;
+                const float W = wab * ww[c][2];
+                float val[4] = {W * mass, W * (part[0] + S[0][2] * dz), W * (part[1] + S[1][2] * dz),
+                                W * (part[2] + S[2][2] * dz)};
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const float o = __shfl_down_sync(0xffffffffu, val[q], 1);
+                    if (absorb) val[q] += o;
+                }
+                if (!active || absorbed) continue;
                 if (!inside && !node_inside(P, base[0] + a, base[1] + b, base[2] + c)) continue;
                 atomicAdd(acc + (ib + c), make_float4(val[0], val[1], val[2], val[3]));
             }
@@ -541,11 +674,16 @@ __global__ void __launch_bounds__(256) k_p2g_mixed(DevParams P, MixedState s, in
 // Fused G2P (this step) -> P2G (next step). do_p2g = 0 gives a plain G2P.
 // SCATTER: 0 = warp-reduced direct float4 atomics, 1 = direct float4
 // atomics, 2 = FP32 shared-memory tile, 3 = int32 fixed-point shared-memory
-// tile (2 and 3 fall back to 0 when the box is too big)
-template <int MINB, int SCATTER>
+// tile (2 and 3 fall back to 0 when the box is too big), 4 = direct float4
+// atomics with same-cell pairs merged. GATHER: 0 = from the grid through
+// L1, 1 = from the warp's velocity box staged in shared memory (dynamic
+// shared memory of 4 x kVBoxNodes float4; SCATTER 0, 1, 4 only).
+constexpr int kVBoxNodes = 256;
+template <int MINB, int SCATTER, int GATHER = 0>
 __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedState s, int n,
                                                            const float4* __restrict__ vel, float4* __restrict__ acc,
-                                                           int do_p2g, int record_pq, int* err, int tile_cap) {
+                                                           int do_p2g, int record_pq, int store_vc, int* err,
+                                                           int tile_cap) {
     extern __shared__ float mixed_tile[];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -554,18 +692,27 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     float E[3][3], Jp = 1.f;
     if (active) load_mixed(s, i, X, E, Jp, st);
     active = active && !(st & (int)kDisabled);
+    const int st_in = st;
+    const float jp_in = Jp;
 
-    int base[3];
-    float fx[3], v[3] = {0, 0, 0}, C[3][3];
+    int base[3] = {0, 0, 0};
+    float fx[3] = {1.f, 1.f, 1.f}, v[3] = {0, 0, 0}, C[3][3];
     bool inside = false;
     ElasticInv inv;
+    int e0 = 0;
     if (active) {
 #pragma unroll
         for (int d = 0; d < 3; d++) fix_base(X[d], base[d], fx[d]);
-        const int e = stencil_error(P, base[0], base[1], base[2]);
-        if (e) raise_error(err, e);
-        g2p_gather_mixed(P, vel, base, fx, v, C, e != 0);
-
+        e0 = stencil_error(P, base[0], base[1], base[2]);
+        if (e0) raise_error(err, e0);
+    }
+    if (GATHER == 1) {
+        float4* vbox = reinterpret_cast<float4*>(mixed_tile) + (threadIdx.x >> 5) * kVBoxNodes;
+        g2p_gather_staged<kVBoxNodes>(P, vel, vbox, active && e0 == 0, active, base, fx, v, C, lane);
+    } else if (active) {
+        g2p_gather_mixed(P, vel, base, fx, v, C, e0 != 0);
+    }
+    if (active) {
         // advection in fixed point, F <- (I + dt C) F as E <- E + dt C (I + E)
         const float dt = (float)P.dt;
         const float adv = dt * (float)P.h_inv * kFixScale;
@@ -610,21 +757,26 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
                 inv = elastic_invariants(E);
             }
         }
-        // store state
+        // store state. v and C are recomputed from the grid by the next G2P
+        // and this launch's P2G takes them from registers, so they are
+        // written only when a reader follows (store_vc: download, sort, the
+        // standalone P2G); Jp_inv and the status word only when they change.
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            s.X[d * s.pitch + i] = X[d];
-            s.v[d * s.pitch + i] = v[d];
-        }
+        for (int d = 0; d < 3; d++) s.X[d * s.pitch + i] = X[d];
 #pragma unroll
         for (int r = 0; r < 3; r++)
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                s.E[(3 * r + c) * s.pitch + i] = E[r][c];
-                s.C[(3 * r + c) * s.pitch + i] = C[r][c];
-            }
-        s.Jp[i] = Jp;
-        s.status[i] = st;
+            for (int c = 0; c < 3; c++) s.E[(3 * r + c) * s.pitch + i] = E[r][c];
+        if (store_vc) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) s.v[d * s.pitch + i] = v[d];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) s.C[(3 * r + c) * s.pitch + i] = C[r][c];
+        }
+        if (__float_as_int(Jp) != __float_as_int(jp_in)) s.Jp[i] = Jp;
+        if (st != st_in) s.status[i] = st;
         if (record_pq) {
             s.PQ[i] = p_tr;
             s.PQ[s.pitch + i] = q_tr;
@@ -665,7 +817,8 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     if (SCATTER == 3 && p2g_scatter_tile_fx<128>(P, acc, reinterpret_cast<int*>(mixed_tile), tile_cap, active, inside,
                                                  base, fx, mass, mv, S, lane))
         return;
-    if (SCATTER == 1) p2g_scatter_mixed<false>(P, acc, active, inside, base, fx, mass, mv, S, lane);
+    if (SCATTER == 4) p2g_scatter_pairs(P, acc, active, inside, base, fx, mass, mv, S, lane);
+    else if (SCATTER == 1) p2g_scatter_mixed<false>(P, acc, active, inside, base, fx, mass, mv, S, lane);
     else p2g_scatter_mixed<true>(P, acc, active, inside, base, fx, mass, mv, S, lane);
 }
 

@@ -81,7 +81,8 @@ struct mpm_handle {
     float4* gvel = nullptr;
     bool p2g_ready = false;           // gacc holds the P2G of the current state
     int mixed_variant = 2;            // fused kernel occupancy target (test hook)
-    int mixed_scatter = 1;            // fused kernel scatter: 0 warp-reduced, 1 direct (default), 2 tile (test hook)
+    int mixed_scatter = 4;            // fused kernel scatter: 0 warp-reduced, 1 direct, 2/3 tiles, 4 pairs (default)
+    int mixed_gather = 1;             // fused kernel gather: 0 through L1, 1 staged warp box (default)
 
     // adjoint (FP64 modes): checkpoints of the recorded forward run
     std::vector<double*> ckpt;        // particle state at substeps 0, k, 2k, ...
@@ -304,18 +305,41 @@ int launch_update(mpm_handle* h, double ind_x, double ind_y, double* force3) {
     return MPM_OK;
 }
 
-int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq) {
+// store_vc: write v and C to the state (needed before a download, a sort or a
+// standalone P2G; the fused chain itself does not read them back).
+int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
     const int n = (int)h->n;
     if (n == 0) return MPM_OK;
     const unsigned nb = blocks_for(n, 128);
-    const size_t tsm = h->mixed_scatter >= 2 ? sizeof(float) * 4 * kMixedTileNodes : 0;
+    const int sc = h->mixed_scatter;
+    if (h->mixed_gather) {
+        // staged gather: 4 warps x kVBoxNodes float4 of dynamic shared memory
+        const size_t vsm = sizeof(float4) * 4 * kVBoxNodes;
+#define FUSED_G(MINB, SC)                                                                                           \
+    k_g2p2g_mixed<MINB, SC, 1><<<nb, 128, vsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,    \
+                                                            record_pq, store_vc, h->err, 0)
+        if (h->mixed_variant == 1) {
+            if (sc == 4) FUSED_G(5, 4);
+            else if (sc == 0) FUSED_G(5, 0);
+            else FUSED_G(5, 1);
+        } else {
+            if (sc == 4) FUSED_G(6, 4);
+            else if (sc == 0) FUSED_G(6, 0);
+            else FUSED_G(6, 1);
+        }
+#undef FUSED_G
+        CK_LAUNCH(h, "g2p2g mixed (staged gather)");
+        return MPM_OK;
+    }
+    const size_t tsm = (sc == 2 || sc == 3) ? sizeof(float) * 4 * kMixedTileNodes : 0;
 #define FUSED(MINB, SC)                                                                                          \
     k_g2p2g_mixed<MINB, SC><<<nb, 128, tsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,     \
-                                                         record_pq, h->err, kMixedTileNodes)
-#define FUSED_SC(MINB)                              \
-    if (h->mixed_scatter == 3) FUSED(MINB, 3);      \
-    else if (h->mixed_scatter == 2) FUSED(MINB, 2); \
-    else if (h->mixed_scatter == 1) FUSED(MINB, 1); \
+                                                         record_pq, store_vc, h->err, kMixedTileNodes)
+#define FUSED_SC(MINB)                  \
+    if (sc == 4) FUSED(MINB, 4);        \
+    else if (sc == 3) FUSED(MINB, 3);   \
+    else if (sc == 2) FUSED(MINB, 2);   \
+    else if (sc == 1) FUSED(MINB, 1);   \
     else FUSED(MINB, 0);
     if (h->mixed_variant == 1) { FUSED_SC(5) }
     else if (h->mixed_variant == 2) { FUSED_SC(6) }
@@ -329,7 +353,7 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq) {
 int launch_g2p(mpm_handle* h, int record_pq) {
     const int n = (int)h->n;
     if (n == 0) return MPM_OK;
-    if (is_mixed(h)) return launch_g2p2g_mixed(h, 0, record_pq);
+    if (is_mixed(h)) return launch_g2p2g_mixed(h, 0, record_pq, 1);
     const unsigned nb = blocks_for(n, 128);
     const bool f32svd = h->precision == MPM_PRECISION_FP64;
 #define G2P_LAUNCH(MINB)                                                                                        \
@@ -730,7 +754,8 @@ int mpm_step(mpm_handle* h, int nsteps, double* force_hist) {
             // the P2G of the next one (the accumulator stays ready)
             if ((r = launch_update(h, p.indenter_x, p.indenter_y, h->force_steps + 3 * s))) return r;
             const int record = (p.SimulationStep % p.UpdateEveryNthStep) == 0;
-            if ((r = launch_g2p2g_mixed(h, 1, record))) return r;
+            const bool sort_next = h->sort_interval > 0 && h->steps_since_sort + 1 >= h->sort_interval;
+            if ((r = launch_g2p2g_mixed(h, 1, record, s == nsteps - 1 || sort_next))) return r;
             p.SimulationStep += 1;
             if (h->sort_interval > 0 && ++h->steps_since_sort >= h->sort_interval) {
                 if ((r = do_sort(h))) return r;
@@ -879,7 +904,7 @@ int mpm_testing_step_timed(mpm_handle* h, int nsteps, float* ms) {
             cudaEventRecord(ev[2], h->stream);
             if ((r = launch_update(h, p.indenter_x, p.indenter_y, h->force_phase))) break;
             cudaEventRecord(ev[3], h->stream);
-            if ((r = launch_g2p2g_mixed(h, 1, record))) break;
+            if ((r = launch_g2p2g_mixed(h, 1, record, s == nsteps - 1))) break;
         } else {
             if ((r = reset_grid(h))) break;
             cudaEventRecord(ev[1], h->stream);
@@ -922,9 +947,16 @@ int mpm_testing_active_nodes(mpm_handle* h, long long* count) {
 }
 
 int mpm_testing_set_g2p_variant(mpm_handle* h, int variant) {
-    if (!h || variant < 0 || variant > 2) return MPM_ERR_ARG;
+    if (!h || variant < 0 || variant > 4) return MPM_ERR_ARG;
+    if (variant >= 3) {
+        if (!is_mixed(h)) return MPM_ERR_ARG;
+        h->mixed_variant = variant == 3 ? 2 : 1;
+        h->mixed_gather = 1;
+        return MPM_OK;
+    }
     h->g2p_variant = variant;
     h->mixed_variant = variant;
+    h->mixed_gather = 0;
     return MPM_OK;
 }
 
@@ -952,7 +984,7 @@ int mpm_testing_download_grid(mpm_handle* h, double* out, int which) {
 }
 
 int mpm_testing_set_p2g_variant(mpm_handle* h, int variant) {
-    if (!h || variant < 0 || variant > 8) return MPM_ERR_ARG;
+    if (!h || variant < 0 || variant > 9) return MPM_ERR_ARG;
     if (variant >= 5) {
         h->mixed_scatter = variant - 5;
         return MPM_OK;

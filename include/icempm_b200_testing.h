@@ -18,13 +18,16 @@ extern "C" {
  * base cell, 3 = as 0 with that warp reduction, 4 = shared-memory tile in
  * 64-bit block fixed point over 1024-particle chunks. In the mixed mode,
  * 5..8 select the fused kernel's scatter: 5 = warp-reduced float4 atomics,
- * 6 = float4 atomics per particle (default), 7 = FP32 shared-memory tile,
- * 8 = int32 block fixed-point shared-memory tile. */
+ * 6 = float4 atomics per particle, 7 = FP32 shared-memory tile,
+ * 8 = int32 block fixed-point shared-memory tile, 9 = float4 atomics with
+ * same-cell particle pairs merged in registers (default). */
 int mpm_testing_set_p2g_variant(mpm_handle* h, int variant);
 
 /* G2P kernel occupancy target (FP64 modes): 0 = 4 blocks of 128 threads per
  * SM, 1 = 3 blocks, 2 = 6 blocks (default; fewer registers per thread). In
- * the mixed mode the fused kernel's target: 0 = 4, 1 = 5, 2 = 6 blocks. */
+ * the mixed mode the fused kernel's target: 0 = 4, 1 = 5, 2 = 6 blocks;
+ * 3 = 6 (default) and 4 = 5 blocks with each warp's velocity box staged in
+ * shared memory for the gather (mixed mode only). */
 int mpm_testing_set_g2p_variant(mpm_handle* h, int variant);
 
 /* Runs the device 3x3 SVD on `count` row-major matrices A (9 doubles each)

@@ -34,13 +34,18 @@ def test_upload_download_round_trip():
     assert np.array_equal(util_bits(out), util_bits(soa))
 
 
-@pytest.mark.parametrize("scatter", [5, 6, 7, 8])
-def test_single_step_phases_close_to_oracle(scatter):
+# (p2g/scatter variant, g2p/gather variant) pairs of the fused kernel
+FUSED_VARIANTS = [(5, 2), (6, 2), (7, 2), (8, 2), (9, 2), (6, 3), (9, 3), (9, 4)]
+
+
+@pytest.mark.parametrize("scatter,gather", FUSED_VARIANTS)
+def test_single_step_phases_close_to_oracle(scatter, gather):
     prms, soa = perturbed_block(n=4000, seed=31)
     n = soa.shape[1]
     ix = prms.indenter_x + 0.02
     with MPMHandle(prms, n, PRECISION_MIXED) as h:
         h.set_p2g_variant(scatter)
+        h.set_g2p_variant(gather)
         h.upload(soa)
         h.reset_indenter_force_accumulator()
         h.reset_grid()
@@ -73,13 +78,14 @@ def test_single_step_phases_close_to_oracle(scatter):
     assert rel_dev(out[IDX_JP_INV][same], ref[IDX_JP_INV][same]) < 1e-5
 
 
-@pytest.mark.parametrize("scatter", [5, 6, 7, 8])
-def test_force_history_within_1e3_of_fp64(scatter):
+@pytest.mark.parametrize("scatter,gather", FUSED_VARIANTS)
+def test_force_history_within_1e3_of_fp64(scatter, gather):
     prms, soa = perturbed_block(n=3000, seed=41, ind_velocity=0.5, crushed_frac=0.05, strong_frac=0.0)
     n = soa.shape[1]
     steps = 60
     with MPMHandle(prms, n, PRECISION_MIXED) as h:
         h.set_p2g_variant(scatter)
+        h.set_g2p_variant(gather)
         h.upload(soa)
         hist = h.step(steps)
         out = h.download()
@@ -106,3 +112,33 @@ def test_sort_in_mixed_mode_matches_oracle_permutation():
     perm = po.sort_permutation(prms, held, n)
     assert np.array_equal(ids, perm)
     assert np.array_equal(out, held[:, perm])
+
+
+def test_split_calls_and_periodic_sort_keep_state():
+    """The fused kernel writes v and C only on the last substep of a call and
+    before a sort; a run split over calls with sorts in between must carry the
+    same state as one call and stay on the FP64 oracle."""
+    prms, soa = perturbed_block(n=3000, seed=43, ind_velocity=0.5, crushed_frac=0.05, strong_frac=0.0)
+    n = soa.shape[1]
+    steps = 30
+    outs = []
+    for chunks in ((30,), (10, 7, 13)):
+        with MPMHandle(prms, n, PRECISION_MIXED) as h:
+            h.upload(soa)
+            h.set_sort_interval(4)
+            hist = np.concatenate([h.step(c) for c in chunks])
+            out = h.download()
+            ids = h.ids()
+        full = np.zeros_like(out)
+        full[:, ids] = out
+        outs.append((hist, full))
+    sim = po.OracleSim(prms, soa, n, svd_mode=1)
+    ref_hist, err = sim.step(steps)
+    assert err == 0
+    for hist, full in outs:
+        assert np.linalg.norm(hist - ref_hist) / np.linalg.norm(ref_hist) < 1e-3
+        assert np.abs(full[POSX:POSX + 3] - sim.soa[POSX:POSX + 3]).max() < 1e-6
+        assert rel_dev(full[VELX:VELX + 3], sim.soa[VELX:VELX + 3]) < 1e-3
+        assert rel_dev(full[BP00:BP00 + 9], sim.soa[BP00:BP00 + 9]) < 1e-3
+    (h1, f1), (h2, f2) = outs
+    assert np.abs(f1[VELX:VELX + 3] - f2[VELX:VELX + 3]).max() < 1e-4 * np.abs(f1[VELX:VELX + 3]).max()
