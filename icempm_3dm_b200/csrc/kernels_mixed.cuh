@@ -683,7 +683,8 @@ template <int MINB, int SCATTER, int GATHER = 0>
 __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedState s, int n,
                                                            const float4* __restrict__ vel, float4* __restrict__ acc,
                                                            int do_p2g, int record_pq, int store_vc, int* err,
-                                                           int tile_cap) {
+                                                           int tile_cap, int* __restrict__ rm_list,
+                                                           int* __restrict__ rm_count) {
     extern __shared__ float mixed_tile[];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -712,6 +713,7 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     } else if (active) {
         g2p_gather_mixed(P, vel, base, fx, v, C, e0 != 0);
     }
+    bool need_rm = false;
     if (active) {
         // advection in fixed point, F <- (I + dt C) F as E <- E + dt C (I + E)
         const float dt = (float)P.dt;
@@ -744,30 +746,38 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
             inv = elastic_invariants(E);
             trial_pq_inv(P, inv, p_tr, q_tr);
             if (!(st & (int)kCrushed) && outside_failure_surface_f32(P, (short)st, p_tr, q_tr)) st |= (int)kCrushed;
-            if (st & (int)kCrushed) {
-                const double p0 = s.p0 ? (double)s.p0[i] : P.p0;
-                ElasticState es;
-#pragma unroll
-                for (int k = 0; k < 9; k++) es.e[k] = E[k / 3][k % 3];
-                es.jp = Jp;
-                es = return_map_f64(dp_params(P), es, p0);
-#pragma unroll
-                for (int k = 0; k < 9; k++) E[k / 3][k % 3] = es.e[k];
-                Jp = es.jp;
-                inv = elastic_invariants(E);
-            }
+            need_rm = (st & (int)kCrushed) != 0;
         }
+        if (record_pq) {
+            s.PQ[i] = p_tr;
+            s.PQ[s.pitch + i] = q_tr;
+        }
+    }
+    // Crushed points leave the fused path here: their trial state is stored
+    // (v and C included) and their index appended to rm_list; the return map
+    // and their P2G run in k_return_map_mixed. No call in this kernel keeps
+    // its register allocation free of the call's save/restore traffic.
+    const unsigned rm_mask = __ballot_sync(0xffffffffu, need_rm);
+    if (rm_mask) {
+        const int first = __ffs(rm_mask) - 1;
+        int slot0 = 0;
+        if (lane == first) slot0 = atomicAdd(rm_count, __popc(rm_mask));
+        slot0 = __shfl_sync(0xffffffffu, slot0, first);
+        if (need_rm) rm_list[slot0 + __popc(rm_mask & ((1u << lane) - 1u))] = i;
+    }
+    if (active) {
         // store state. v and C are recomputed from the grid by the next G2P
         // and this launch's P2G takes them from registers, so they are
         // written only when a reader follows (store_vc: download, sort, the
-        // standalone P2G); Jp_inv and the status word only when they change.
+        // standalone P2G, the return-map kernel); Jp_inv and the status word
+        // only when they change.
 #pragma unroll
         for (int d = 0; d < 3; d++) s.X[d * s.pitch + i] = X[d];
 #pragma unroll
         for (int r = 0; r < 3; r++)
 #pragma unroll
             for (int c = 0; c < 3; c++) s.E[(3 * r + c) * s.pitch + i] = E[r][c];
-        if (store_vc) {
+        if (store_vc || need_rm) {
 #pragma unroll
             for (int d = 0; d < 3; d++) s.v[d * s.pitch + i] = v[d];
 #pragma unroll
@@ -777,11 +787,8 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
         }
         if (__float_as_int(Jp) != __float_as_int(jp_in)) s.Jp[i] = Jp;
         if (st != st_in) s.status[i] = st;
-        if (record_pq) {
-            s.PQ[i] = p_tr;
-            s.PQ[s.pitch + i] = q_tr;
-        }
     }
+    active = active && !need_rm;   // crushed points scatter in k_return_map_mixed
     if (!do_p2g) return;   // uniform across the launch
     float mass = 0.f, mv[3] = {0, 0, 0}, S[3][3];
     if (active) {
@@ -820,6 +827,49 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     if (SCATTER == 4) p2g_scatter_pairs(P, acc, active, inside, base, fx, mass, mv, S, lane);
     else if (SCATTER == 1) p2g_scatter_mixed<false>(P, acc, active, inside, base, fx, mass, mv, S, lane);
     else p2g_scatter_mixed<true>(P, acc, active, inside, base, fx, mass, mv, S, lane);
+}
+
+// Return map (FP64, mpm_kernels.cuh:486-544) of the crushed points listed by
+// k_g2p2g_mixed, then their P2G (direct float4 atomics) when do_p2g. The
+// list holds *count indices; the kernel also clears next_count, the counter
+// the next fused launch appends to. Grid-stride over the list.
+__global__ void __launch_bounds__(128) k_return_map_mixed(DevParams P, MixedState s, const int* __restrict__ rm_list,
+                                                          const int* __restrict__ count, int* __restrict__ next_count,
+                                                          float4* __restrict__ acc, int do_p2g, int* err) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *next_count = 0;
+    const int m = *count;
+    const int lane = threadIdx.x & 31;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const int i = rm_list[k];
+        int X[3], st;
+        float E[3][3], Jp;
+        load_mixed(s, i, X, E, Jp, st);
+        const double p0 = s.p0 ? (double)s.p0[i] : P.p0;
+        ElasticState es;
+#pragma unroll
+        for (int q = 0; q < 9; q++) es.e[q] = E[q / 3][q % 3];
+        es.jp = Jp;
+        es = return_map_f64(dp_params(P), es, p0);
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            E[q / 3][q % 3] = es.e[q];
+            s.E[q * s.pitch + i] = es.e[q];
+        }
+        if (__float_as_int(es.jp) != __float_as_int(Jp)) s.Jp[i] = es.jp;
+        if (!do_p2g) continue;
+        float v[3], C[3][3], mass, mv[3], S[3][3], fx[3];
+        int base[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) v[d] = s.v[d * s.pitch + i];
+#pragma unroll
+        for (int q = 0; q < 9; q++) C[q / 3][q % 3] = s.C[q * s.pitch + i];
+#pragma unroll
+        for (int d = 0; d < 3; d++) fix_base(X[d], base[d], fx[d]);
+        p2g_payload_mixed(P, E, C, v, false, es.jp, mass, mv, S);
+        const int e = stencil_error(P, base[0], base[1], base[2]);
+        if (e) raise_error(err, e);
+        p2g_scatter_mixed<false>(P, acc, true, e == 0, base, fx, mass, mv, S, lane);
+    }
 }
 
 // Node update for the mixed grid: FP64 arithmetic on the FP32 sums, contact

@@ -80,9 +80,12 @@ struct mpm_handle {
     float4* gacc = nullptr;
     float4* gvel = nullptr;
     bool p2g_ready = false;           // gacc holds the P2G of the current state
-    int mixed_variant = 2;            // fused kernel occupancy target (test hook)
+    int mixed_variant = 3;            // fused kernel occupancy target: 3 = 8 blocks of 128 per SM (test hook)
     int mixed_scatter = 4;            // fused kernel scatter: 0 warp-reduced, 1 direct, 2/3 tiles, 4 pairs (default)
     int mixed_gather = 1;             // fused kernel gather: 0 through L1, 1 staged warp box (default)
+    int* rm_list = nullptr;           // crushed points deferred to k_return_map_mixed (n entries)
+    int* rm_counts = nullptr;         // two list counters, used alternately by successive launches
+    int rm_parity = 0;
 
     // adjoint (FP64 modes): checkpoints of the recorded forward run
     std::vector<double*> ckpt;        // particle state at substeps 0, k, 2k, ...
@@ -189,6 +192,7 @@ void free_all(mpm_handle* h) {
     cudaFree(h->s_bucket); cudaFree(h->s_count); cudaFree(h->s_start); cudaFree(h->s_perm);
     cudaFree(h->chunk_bound);
     cudaFree(h->mx); cudaFree(h->p0f); cudaFree(h->gacc); cudaFree(h->gvel);
+    cudaFree(h->rm_list); cudaFree(h->rm_counts);
     for (double* c : h->ckpt) cudaFree(c);
     for (double* c : h->seg) cudaFree(c);
     h->ckpt.clear();
@@ -268,12 +272,6 @@ int launch_p2g(mpm_handle* h) {
             const int chunks = (int)blocks_for(n, kFxBlock * kFxPPT);
             if (chunks > h->chunk_bound_cap) {
                 cudaFree(h->chunk_bound);
-    cudaFree(h->mx); cudaFree(h->p0f); cudaFree(h->gacc); cudaFree(h->gvel);
-    for (double* c : h->ckpt) cudaFree(c);
-    for (double* c : h->seg) cudaFree(c);
-    h->ckpt.clear();
-    h->seg.clear();
-    cudaFree(h->adj_A); cudaFree(h->adj_cgrad); cudaFree(h->adj_Egrad); cudaFree(h->adj_g7); cudaFree(h->adj_gb7);
                 h->chunk_bound = nullptr;
                 CK(h, cudaMalloc(&h->chunk_bound, sizeof(float) * chunks));
                 CK(h, cudaMemsetAsync(h->chunk_bound, 0, sizeof(float) * chunks, h->stream));
@@ -305,6 +303,17 @@ int launch_update(mpm_handle* h, double ind_x, double ind_y, double* force3) {
     return MPM_OK;
 }
 
+// Return map and P2G of the crushed points the last fused launch listed
+// (one persistent grid of 4 blocks per SM walks the list).
+int launch_return_map_mixed(mpm_handle* h, int do_p2g) {
+    const int cur = h->rm_parity;
+    h->rm_parity ^= 1;
+    k_return_map_mixed<<<148 * 4, 128, 0, h->stream>>>(h->dp, mixed_state(h), h->rm_list, h->rm_counts + cur,
+                                                       h->rm_counts + (cur ^ 1), h->gacc, do_p2g, h->err);
+    CK_LAUNCH(h, "return map mixed");
+    return MPM_OK;
+}
+
 // store_vc: write v and C to the state (needed before a download, a sort or a
 // standalone P2G; the fused chain itself does not read them back).
 int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
@@ -312,16 +321,20 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
     if (n == 0) return MPM_OK;
     const unsigned nb = blocks_for(n, 128);
     const int sc = h->mixed_scatter;
+    int* const rm_count = h->rm_counts + h->rm_parity;
     if (h->mixed_gather) {
         // staged gather: 4 warps x kVBoxNodes float4 of dynamic shared memory
         const size_t vsm = sizeof(float4) * 4 * kVBoxNodes;
 #define FUSED_G(MINB, SC)                                                                                           \
     k_g2p2g_mixed<MINB, SC, 1><<<nb, 128, vsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,    \
-                                                            record_pq, store_vc, h->err, 0)
+                                                            record_pq, store_vc, h->err, 0, h->rm_list, rm_count)
         if (h->mixed_variant == 1) {
             if (sc == 4) FUSED_G(5, 4);
             else if (sc == 0) FUSED_G(5, 0);
             else FUSED_G(5, 1);
+        } else if (h->mixed_variant == 3) {
+            if (sc == 4) FUSED_G(8, 4);
+            else FUSED_G(8, 1);
         } else {
             if (sc == 4) FUSED_G(6, 4);
             else if (sc == 0) FUSED_G(6, 0);
@@ -329,12 +342,13 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
         }
 #undef FUSED_G
         CK_LAUNCH(h, "g2p2g mixed (staged gather)");
-        return MPM_OK;
+        return launch_return_map_mixed(h, do_p2g);
     }
     const size_t tsm = (sc == 2 || sc == 3) ? sizeof(float) * 4 * kMixedTileNodes : 0;
 #define FUSED(MINB, SC)                                                                                          \
     k_g2p2g_mixed<MINB, SC><<<nb, 128, tsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,     \
-                                                         record_pq, store_vc, h->err, kMixedTileNodes)
+                                                         record_pq, store_vc, h->err, kMixedTileNodes, h->rm_list,  \
+                                                         rm_count)
 #define FUSED_SC(MINB)                  \
     if (sc == 4) FUSED(MINB, 4);        \
     else if (sc == 3) FUSED(MINB, 3);   \
@@ -347,7 +361,7 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
 #undef FUSED_SC
 #undef FUSED
     CK_LAUNCH(h, "g2p2g mixed");
-    return MPM_OK;
+    return launch_return_map_mixed(h, do_p2g);
 }
 
 int launch_g2p(mpm_handle* h, int record_pq) {
@@ -555,10 +569,13 @@ mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity
         if (precision == MPM_PRECISION_MIXED) {
             if (cudaMalloc(&h->mx, sizeof(float) * MPM_N_PTS_ARRAYS * h->pitch) != cudaSuccess ||
                 cudaMalloc(&h->gacc, sizeof(float4) * (size_t)h->dp.nodes) != cudaSuccess ||
-                cudaMalloc(&h->gvel, sizeof(float4) * (size_t)h->dp.nodes) != cudaSuccess) {
+                cudaMalloc(&h->gvel, sizeof(float4) * (size_t)h->dp.nodes) != cudaSuccess ||
+                cudaMalloc(&h->rm_list, sizeof(int) * h->pitch) != cudaSuccess ||
+                cudaMalloc(&h->rm_counts, sizeof(int) * 2) != cudaSuccess) {
                 st = MPM_ERR_CUDA;
                 break;
             }
+            cudaMemsetAsync(h->rm_counts, 0, sizeof(int) * 2, h->stream);
             cudaMemsetAsync(h->mx, 0, sizeof(float) * MPM_N_PTS_ARRAYS * h->pitch, h->stream);
             cudaMemsetAsync(h->gacc, 0, sizeof(float4) * (size_t)h->dp.nodes, h->stream);
             cudaMemsetAsync(h->gvel, 0, sizeof(float4) * (size_t)h->dp.nodes, h->stream);
@@ -947,10 +964,10 @@ int mpm_testing_active_nodes(mpm_handle* h, long long* count) {
 }
 
 int mpm_testing_set_g2p_variant(mpm_handle* h, int variant) {
-    if (!h || variant < 0 || variant > 4) return MPM_ERR_ARG;
+    if (!h || variant < 0 || variant > 5) return MPM_ERR_ARG;
     if (variant >= 3) {
         if (!is_mixed(h)) return MPM_ERR_ARG;
-        h->mixed_variant = variant == 3 ? 2 : 1;
+        h->mixed_variant = variant == 3 ? 2 : variant == 4 ? 1 : 3;
         h->mixed_gather = 1;
         return MPM_OK;
     }
