@@ -149,15 +149,37 @@ __device__ __forceinline__ void trial_pq_mixed(const DevParams& P, const float E
     q_tr = (float)(kCoeff1 * P.mu) * exp2f(-(2.0f / 3.0f) * log2f(J)) * sqrtf(sq);
 }
 
+// w[a] of a 3-entry weight column with a loop counter that is not unrolled:
+// selects keep the column in registers (an indexed load would place the
+// whole weight array in local memory).
+__device__ __forceinline__ float pick3(int a, float w0, float w1, float w2) {
+    return a == 0 ? w0 : (a == 1 ? w1 : w2);
+}
+
+// The x-column of the weights in a per-thread shared-memory slot (stride
+// 128 floats): read with the loop counter of a loop that is not unrolled, it
+// costs one shared load per iteration and no register (local memory would
+// also send its stores on to L2).
+struct WxSlot {
+    float* p;
+    __device__ __forceinline__ void put(const float ww[3][3]) {
+        p[0] = ww[0][0];
+        p[128] = ww[1][0];
+        p[256] = ww[2][0];
+    }
+    __device__ __forceinline__ float get(int a) const { return *(volatile const float*)(p + 128 * a); }
+};
+
 // ------------------------------------------------------------- G2P part
 
 // Gathers v and C from the float4 velocity grid (mpm_kernels.cuh:278-305).
 // Node indices step from the base node by constant offsets (32-bit: the
 // handle checks that the grid has fewer than 2^31 nodes).
 __device__ __forceinline__ void g2p_gather_mixed(const DevParams& P, const float4* __restrict__ vel, const int base[3],
-                                                 const float fx[3], float v[3], float C[3][3], bool check) {
+                                                 const float fx[3], float v[3], float C[3][3], bool check, WxSlot wx) {
     float ww[3][3];
     quad_weights<float>(fx, ww);
+    wx.put(ww);
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         v[d] = 0.f;
@@ -169,7 +191,7 @@ __device__ __forceinline__ void g2p_gather_mixed(const DevParams& P, const float
     const int i0 = ((base[0] + P.halo) * P.Gy + base[1]) * gz + base[2];
 #pragma unroll 1
     for (int a = 0; a < 3; a++) {
-        const float wa = ww[a][0];
+        const float wa = wx.get(a);
         const float dpa = a - fx[0];
 #pragma unroll
         for (int b = 0; b < 3; b++) {
@@ -207,7 +229,7 @@ template <int VCAP>
 __device__ __forceinline__ void g2p_gather_staged(const DevParams& P, const float4* __restrict__ vel,
                                                   float4* __restrict__ vbox, bool part, bool active,
                                                   const int base[3], const float fx[3], float v[3], float C[3][3],
-                                                  int lane) {
+                                                  int lane, WxSlot wx) {
     const int lo0 = __reduce_min_sync(0xffffffffu, part ? base[0] : INT_MAX);
     const int lo1 = __reduce_min_sync(0xffffffffu, part ? base[1] : INT_MAX);
     const int lo2 = __reduce_min_sync(0xffffffffu, part ? base[2] : INT_MAX);
@@ -237,44 +259,60 @@ __device__ __forceinline__ void g2p_gather_staged(const DevParams& P, const floa
         }
     }
     if (part && staged) {
+        // v = sum w nv and the first moments M_k = sum w nv o_k over the node
+        // offsets o = (a, b, c); C = 4/h sum w nv (o - f) = 4/h (M - f v)
+        // (mpm_kernels.cuh:278-305 summed in this order).
         float ww[3][3];
         quad_weights<float>(fx, ww);
+        wx.put(ww);
+        float Mx[3], My[3], Mz[3];
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            v[d] = 0.f;
-#pragma unroll
-            for (int k = 0; k < 3; k++) C[d][k] = 0.f;
-        }
-        const float s4 = 4.0f * (float)P.h_inv;
+        for (int r = 0; r < 3; r++) { v[r] = 0.f; Mx[r] = 0.f; My[r] = 0.f; Mz[r] = 0.f; }
         const int t0 = ((base[0] - lo0) * ey + (base[1] - lo1)) * ez + (base[2] - lo2);
 #pragma unroll 1
         for (int a = 0; a < 3; a++) {
-            const float wa = ww[a][0];
-            const float dpa = a - fx[0];
+            const float wa = wx.get(a);
+            float ra[3] = {0.f, 0.f, 0.f};
 #pragma unroll
             for (int b = 0; b < 3; b++) {
                 const float wab = wa * ww[b][1];
-                const float dpb = b - fx[1];
-                const int tb = t0 + a * ey * ez + b * ez;
+                const float4* row = vbox + (t0 + a * ey * ez + b * ez);
+                float rb[3] = {0.f, 0.f, 0.f};
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
-                    const float4 nd = vbox[tb + c];
+                    const float4 nd = row[c];
                     const float w = wab * ww[c][2];
-                    const float nv[3] = {nd.x, nd.y, nd.z};
-                    const float dp[3] = {dpa, dpb, c - fx[2]};
-                    const float sw = s4 * w;
+                    const float wn[3] = {w * nd.x, w * nd.y, w * nd.z};
 #pragma unroll
                     for (int r = 0; r < 3; r++) {
-                        v[r] += w * nv[r];
-                        const float swv = sw * nv[r];
-#pragma unroll
-                        for (int k = 0; k < 3; k++) C[r][k] += swv * dp[k];
+                        rb[r] += wn[r];
+                        if (c == 1) Mz[r] += wn[r];
+                        if (c == 2) Mz[r] += 2.0f * wn[r];
                     }
                 }
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    ra[r] += rb[r];
+                    if (b == 1) My[r] += rb[r];
+                    if (b == 2) My[r] += 2.0f * rb[r];
+                }
+            }
+            const float fa = (float)a;
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                v[r] += ra[r];
+                Mx[r] += fa * ra[r];
             }
         }
+        const float s4 = 4.0f * (float)P.h_inv;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            C[r][0] = s4 * (Mx[r] - fx[0] * v[r]);
+            C[r][1] = s4 * (My[r] - fx[1] * v[r]);
+            C[r][2] = s4 * (Mz[r] - fx[2] * v[r]);
+        }
     } else if (active) {
-        g2p_gather_mixed(P, vel, base, fx, v, C, !part);
+        g2p_gather_mixed(P, vel, base, fx, v, C, !part, wx);
     }
     __syncwarp();
 }
@@ -329,7 +367,7 @@ __device__ __forceinline__ void p2g_scatter_mixed(const DevParams& P, float4* __
 #pragma unroll
         for (int b = 0; b < 3; b++) {
             const float dy = (b - fx[1]) * h;
-            const float wab = ww[a][0] * ww[b][1];
+            const float wab = pick3(a, ww[0][0], ww[1][0], ww[2][0]) * ww[b][1];
             const int ib = i0 + a * slab + b * gz;
             float part[3];
 #pragma unroll
@@ -366,7 +404,7 @@ __device__ __forceinline__ void p2g_scatter_mixed(const DevParams& P, float4* __
 // atomic traffic to L2 at ppc ~2 for 8 shuffles and adds per node.
 __device__ __forceinline__ void p2g_scatter_pairs(const DevParams& P, float4* __restrict__ acc, bool active,
                                                   bool inside, const int base[3], const float fx[3], float mass,
-                                                  const float mv[3], const float S[3][3], int lane) {
+                                                  const float mv[3], const float S[3][3], int lane, WxSlot wx) {
     const int i0 = ((base[0] + P.halo) * P.Gy + base[1]) * P.Gz + base[2];
     const int key = (active && inside) ? i0 : -1 - lane;
     const unsigned peers = __match_any_sync(0xffffffffu, key);
@@ -376,15 +414,51 @@ __device__ __forceinline__ void p2g_scatter_pairs(const DevParams& P, float4* __
     const bool absorbed = __shfl_up_sync(0xffffffffu, (int)absorb, 1) != 0 && lane > 0;
     float ww[3][3];
     quad_weights<float>(fx, ww);
+    wx.put(ww);
+    const bool emit = active && !absorbed;
+    if (__all_sync(0xffffffffu, inside || !active)) {
+        // every stencil of the warp lies in the grid: no per-node checks
+        const float h = (float)P.h;
+        const int slab = (int)P.slab, gz = P.Gz;
+#pragma unroll 1
+        for (int a = 0; a < 3; a++) {
+            const float dx = (a - fx[0]) * h;
+            const float wa = wx.get(a);
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                const float dy = (b - fx[1]) * h;
+                const float wab = wa * ww[b][1];
+                const int ib = i0 + a * slab + b * gz;
+                float part[3];
+#pragma unroll
+                for (int m = 0; m < 3; m++) part[m] = mv[m] + S[m][0] * dx + S[m][1] * dy;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const float dz = (c - fx[2]) * h;
+                    const float W = wab * ww[c][2];
+                    float val[4] = {W * mass, W * (part[0] + S[0][2] * dz), W * (part[1] + S[1][2] * dz),
+                                    W * (part[2] + S[2][2] * dz)};
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float o = __shfl_down_sync(0xffffffffu, val[q], 1);
+                        if (absorb) val[q] += o;
+                    }
+                    if (emit) atomicAdd(acc + (ib + c), make_float4(val[0], val[1], val[2], val[3]));
+                }
+            }
+        }
+        return;
+    }
     const float h = (float)P.h;
     const int slab = (int)P.slab, gz = P.Gz;
 #pragma unroll 1
     for (int a = 0; a < 3; a++) {
         const float dx = (a - fx[0]) * h;
+        const float wa = wx.get(a);
 #pragma unroll
         for (int b = 0; b < 3; b++) {
             const float dy = (b - fx[1]) * h;
-            const float wab = ww[a][0] * ww[b][1];
+            const float wab = wa * ww[b][1];
             const int ib = i0 + a * slab + b * gz;
             float part[3];
 #pragma unroll
@@ -455,7 +529,7 @@ __device__ __forceinline__ bool p2g_scatter_tile(const DevParams& P, float4* __r
 #pragma unroll
             for (int b = 0; b < 3; b++) {
                 const float dy = (b - fx[1]) * h;
-                const float wab = ww[a][0] * ww[b][1];
+                const float wab = pick3(a, ww[0][0], ww[1][0], ww[2][0]) * ww[b][1];
                 const int tb = t0 + (a * ey + b) * ez;
                 float part[3];
 #pragma unroll
@@ -567,7 +641,7 @@ __device__ __forceinline__ bool p2g_scatter_tile_fx(const DevParams& P, float4* 
 #pragma unroll
             for (int b = 0; b < 3; b++) {
                 const float dy = (b - fx[1]) * h;
-                const float wab = ww[a][0] * ww[b][1];
+                const float wab = pick3(a, ww[0][0], ww[1][0], ww[2][0]) * ww[b][1];
                 const int tb = t0 + (a * ey + b) * ez;
                 float part[3];
 #pragma unroll
@@ -686,6 +760,8 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
                                                            int tile_cap, int* __restrict__ rm_list,
                                                            int* __restrict__ rm_count) {
     extern __shared__ float mixed_tile[];
+    __shared__ float wx_slots[3 * 128];
+    const WxSlot wx{wx_slots + threadIdx.x};
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     bool active = i < n;
@@ -709,9 +785,9 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     }
     if (GATHER == 1) {
         float4* vbox = reinterpret_cast<float4*>(mixed_tile) + (threadIdx.x >> 5) * kVBoxNodes;
-        g2p_gather_staged<kVBoxNodes>(P, vel, vbox, active && e0 == 0, active, base, fx, v, C, lane);
+        g2p_gather_staged<kVBoxNodes>(P, vel, vbox, active && e0 == 0, active, base, fx, v, C, lane, wx);
     } else if (active) {
-        g2p_gather_mixed(P, vel, base, fx, v, C, e0 != 0);
+        g2p_gather_mixed(P, vel, base, fx, v, C, e0 != 0, wx);
     }
     bool need_rm = false;
     if (active) {
@@ -824,7 +900,7 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     if (SCATTER == 3 && p2g_scatter_tile_fx<128>(P, acc, reinterpret_cast<int*>(mixed_tile), tile_cap, active, inside,
                                                  base, fx, mass, mv, S, lane))
         return;
-    if (SCATTER == 4) p2g_scatter_pairs(P, acc, active, inside, base, fx, mass, mv, S, lane);
+    if (SCATTER == 4) p2g_scatter_pairs(P, acc, active, inside, base, fx, mass, mv, S, lane, wx);
     else if (SCATTER == 1) p2g_scatter_mixed<false>(P, acc, active, inside, base, fx, mass, mv, S, lane);
     else p2g_scatter_mixed<true>(P, acc, active, inside, base, fx, mass, mv, S, lane);
 }

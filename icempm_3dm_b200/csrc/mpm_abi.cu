@@ -314,8 +314,10 @@ int launch_return_map_mixed(mpm_handle* h, int do_p2g) {
     return MPM_OK;
 }
 
-// store_vc: write v and C to the state (needed before a download, a sort or a
-// standalone P2G; the fused chain itself does not read them back).
+// Fused G2P -> P2G of all particles but the crushed ones, which it lists for
+// launch_return_map_mixed (the caller launches that next, on the same
+// stream). store_vc: write v and C to the state (needed before a download, a
+// sort or a standalone P2G; the fused chain itself does not read them back).
 int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
     const int n = (int)h->n;
     if (n == 0) return MPM_OK;
@@ -342,7 +344,7 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
         }
 #undef FUSED_G
         CK_LAUNCH(h, "g2p2g mixed (staged gather)");
-        return launch_return_map_mixed(h, do_p2g);
+        return MPM_OK;
     }
     const size_t tsm = (sc == 2 || sc == 3) ? sizeof(float) * 4 * kMixedTileNodes : 0;
 #define FUSED(MINB, SC)                                                                                          \
@@ -361,13 +363,16 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
 #undef FUSED_SC
 #undef FUSED
     CK_LAUNCH(h, "g2p2g mixed");
-    return launch_return_map_mixed(h, do_p2g);
+    return MPM_OK;
 }
 
 int launch_g2p(mpm_handle* h, int record_pq) {
     const int n = (int)h->n;
     if (n == 0) return MPM_OK;
-    if (is_mixed(h)) return launch_g2p2g_mixed(h, 0, record_pq, 1);
+    if (is_mixed(h)) {
+        int r = launch_g2p2g_mixed(h, 0, record_pq, 1);
+        return r ? r : launch_return_map_mixed(h, 0);
+    }
     const unsigned nb = blocks_for(n, 128);
     const bool f32svd = h->precision == MPM_PRECISION_FP64;
 #define G2P_LAUNCH(MINB)                                                                                        \
@@ -773,6 +778,7 @@ int mpm_step(mpm_handle* h, int nsteps, double* force_hist) {
             const int record = (p.SimulationStep % p.UpdateEveryNthStep) == 0;
             const bool sort_next = h->sort_interval > 0 && h->steps_since_sort + 1 >= h->sort_interval;
             if ((r = launch_g2p2g_mixed(h, 1, record, s == nsteps - 1 || sort_next))) return r;
+            if ((r = launch_return_map_mixed(h, 1))) return r;
             p.SimulationStep += 1;
             if (h->sort_interval > 0 && ++h->steps_since_sort >= h->sort_interval) {
                 if ((r = do_sort(h))) return r;
@@ -901,8 +907,8 @@ size_t mpm_testing_sizeof_params(void) { return sizeof(SimParams3D); }
 int mpm_testing_step_timed(mpm_handle* h, int nsteps, float* ms) {
     if (!h || nsteps <= 0 || !ms) return MPM_ERR_ARG;
     if (!h->uploaded) return MPM_ERR_STATE;
-    cudaEvent_t ev[5];
-    for (int k = 0; k < 5; k++) CK(h, cudaEventCreate(&ev[k]));
+    cudaEvent_t ev[6];
+    for (int k = 0; k < 6; k++) CK(h, cudaEventCreate(&ev[k]));
     for (int k = 0; k < 4; k++) ms[k] = 0.f;
     SimParams3D& p = h->prms;
     int r = MPM_OK;
@@ -917,11 +923,23 @@ int mpm_testing_step_timed(mpm_handle* h, int nsteps, float* ms) {
         const int record = (p.SimulationStep % p.UpdateEveryNthStep) == 0;
         cudaEventRecord(ev[0], h->stream);
         if (is_mixed(h)) {
-            cudaEventRecord(ev[1], h->stream);
-            cudaEventRecord(ev[2], h->stream);
+            // ms[0] = 0, ms[1] = return-map kernel, ms[2] = update, ms[3] = fused kernel
             if ((r = launch_update(h, p.indenter_x, p.indenter_y, h->force_phase))) break;
-            cudaEventRecord(ev[3], h->stream);
+            cudaEventRecord(ev[1], h->stream);
             if ((r = launch_g2p2g_mixed(h, 1, record, s == nsteps - 1))) break;
+            cudaEventRecord(ev[2], h->stream);
+            if ((r = launch_return_map_mixed(h, 1))) break;
+            cudaEventRecord(ev[3], h->stream);
+            CK(h, cudaEventSynchronize(ev[3]));
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[0], ev[1]);
+            ms[2] += t;
+            cudaEventElapsedTime(&t, ev[1], ev[2]);
+            ms[3] += t;
+            cudaEventElapsedTime(&t, ev[2], ev[3]);
+            ms[1] += t;
+            p.SimulationStep += 1;
+            continue;
         } else {
             if ((r = reset_grid(h))) break;
             cudaEventRecord(ev[1], h->stream);
@@ -940,7 +958,7 @@ int mpm_testing_step_timed(mpm_handle* h, int nsteps, float* ms) {
         }
         p.SimulationStep += 1;
     }
-    for (int k = 0; k < 5; k++) cudaEventDestroy(ev[k]);
+    for (int k = 0; k < 6; k++) cudaEventDestroy(ev[k]);
     return r;
 }
 

@@ -46,7 +46,8 @@ int mpm_testing_download_grid(mpm_handle* h, double* out, int which);
 /* Runs nsteps substeps like mpm_step (without the force history) with CUDA
  * events recorded on the handle's stream around each kernel; ms[0..3]
  * receive the summed durations of [grid clear, P2G, node update, G2P] (FP64
- * modes) or [-, -, node update, fused G2P->P2G] (mixed mode). */
+ * modes) or [-, return map of crushed points, node update, fused
+ * G2P->P2G] (mixed mode). */
 int mpm_testing_step_timed(mpm_handle* h, int nsteps, float* ms);
 
 /* Number of grid nodes with non-zero mass in the current P2G result (the
