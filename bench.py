@@ -138,17 +138,16 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def traffic_per_particle(kernel, precision):
+def traffic_per_particle(kernel):
     """DRAM bytes per particle of the dominant kernel from the committed ncu
-    summary (profiles/), captured on a smaller block and scaled by particles."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}_{precision}.txt")
-    try:
+    summary profiles/<kernel>_<workload>.md (line `dram_bytes_per_particle:`),
+    captured on a smaller block and scaled by particles."""
+    import glob
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", f"{kernel}_*.md"))):
         with open(path) as f:
             for line in f:
                 if line.startswith("dram_bytes_per_particle:"):
                     return float(line.split(":", 1)[1].split()[0])
-    except OSError:
-        pass
     return None
 
 
@@ -268,7 +267,7 @@ def run_ours(args):
         launches_per_step = 3
     peak, peak_kind = measured_peak_hbm()
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
-    tpp = traffic_per_particle(dom_name, args.precision)
+    tpp = traffic_per_particle(dom_name)
     step_bytes = n * (B_PARTICLE[args.precision] + (B_COHESION[args.precision] if coh is not None else 0)) + \
         active * B_NODE[args.precision]
 
