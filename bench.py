@@ -41,13 +41,14 @@ B_NODE = {"mixed": 32, "fp64": 64}             # bytes per active node per step
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1500)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="block8m")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-seconds", type=float, default=45.0)
     return ap.parse_args()
 
 
@@ -77,7 +78,8 @@ def max_over_ranks(dist, value, device):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks / throttle reasons sampled every 100 ms; stop()
+    keeps the samples that arrived inside the timed window [t0, t1]."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -90,7 +92,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -99,9 +101,9 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
-    def stop(self):
+    def stop(self, t0=None, t1=None):
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -111,7 +113,9 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for t, ln in self.lines:
+            if t0 is not None and not (t0 <= t <= t1):
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -187,17 +191,23 @@ def run_reference(args):
     p0 = None if coh is None else coh / prms.DP_tan_phi
     sim = po.OracleSim(prms, soa, n, p0=p0, svd_mode=0, nthreads=threads)
     sim.step(max(1, min(args.warmup, 3)))
+    # bounded sample: substeps of the full block until --steps are done or
+    # --ref-seconds have elapsed (a CPU substep of the 8M block takes ~0.4 s)
     t0 = time.perf_counter()
-    sim.step(args.steps)
+    done = 0
+    while done < args.steps and (done < 2 or time.perf_counter() - t0 < args.ref_seconds):
+        sim.step(1)
+        done += 1
     dt = time.perf_counter() - t0
-    value = n * args.steps / dt
+    value = n * done / dt
     out = {"impl": "reference", "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
-           "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+           "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / done * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic", "config": {"workload": args.workload, "particles": n},
            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-                            "sample": f"{args.steps} substeps of the full block (oracle port of the reference "
-                                      f"step, FP64, OpenMP)"},
+                            "sample": f"{done} substeps of the full {n}-particle block (oracle port of the "
+                                      f"reference step, FP64, OpenMP {threads} threads; bounded by "
+                                      f"{args.ref_seconds:g} s)"},
            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return 0
@@ -235,14 +245,16 @@ def run_ours(args):
     torch.cuda.synchronize(device)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    t_start = time.monotonic()
     e0.record(stream)
     hist = h.step(args.steps)
     e1.record(stream)
     e1.synchronize()
+    t_end = time.monotonic()
     torch.cuda.synchronize(device)
     if dist is not None:
         dist.barrier()
-    clocks = sampler.stop()
+    clocks = sampler.stop(t_start, t_end)
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(dist, ms, device)
     value = world * n * args.steps / (ms_max * 1e-3)
@@ -258,7 +270,7 @@ def run_ours(args):
             active * B_NODE["mixed"]
         launches_per_step = 3
     else:
-        names = ["grid clear", "k_p2g", "k_update_f64", "k_g2p_f64"]
+        names = ["grid clear", "k_p2g_warpagg_f64", "k_update_f64", "k_g2p_f64"]
         k = int(np.argmax(kms[1:])) + 1
         dom_name, dom_ms = names[k], kms[k] / args.steps
         # FP64 form: P2G reads 200 B (x, v, F, C), G2P reads 112 B and writes 208 B
