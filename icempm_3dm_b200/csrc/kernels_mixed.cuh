@@ -317,6 +317,182 @@ __device__ __forceinline__ void g2p_gather_staged(const DevParams& P, const floa
     __syncwarp();
 }
 
+// ------------------------------------------------- TMA-staged gather box
+// The velocity grid as a 4-D tensor (float components, z, y, x): one tensor
+// copy brings a fixed box of kTmaBoxX x kTmaBoxY x kTmaBoxZ nodes (4,608 B,
+// innermost coordinate 0, so always 16-byte aligned) into the warp's shared
+// slice, completed on a per-warp mbarrier. Plain (non-multicast) loads.
+constexpr int kTmaBoxX = 3, kTmaBoxY = 3, kTmaBoxZ = 20;
+constexpr int kTmaBoxNodes = kTmaBoxX * kTmaBoxY * kTmaBoxZ;
+constexpr unsigned kTmaBoxBytes = kTmaBoxNodes * 16u;
+constexpr int kTmaSliceNodes = 184;   // per-warp slice: >= kTmaBoxNodes, a multiple of 128 B
+constexpr int kTmaWaitPolls = 1 << 22;   // polls of one bounded wait (a copy takes ~1 us)
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init_one(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for phase `parity` of bar: false when kTmaWaitPolls polls passed.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    for (int k = 0; k < kTmaWaitPolls; k++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_box(void* dst, const CUtensorMap* map, int z0, int y0, int x0,
+                                             unsigned long long* bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(0), "r"(z0), "r"(y0), "r"(x0), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Box of base cells of the warp's lanes with an in-grid stencil, and the
+// TMA copy of its velocity nodes when it fits the fixed box (issued by lane
+// 0 as soon as the bases are known, so that it overlaps the particles' other
+// loads). Called by the whole warp.
+struct WarpBox {
+    int lo0, lo1, lo2, ex, ey, ez;
+    bool any, tma;
+};
+
+__device__ __forceinline__ WarpBox warp_box_issue(const DevParams& P, const CUtensorMap* map, float4* vbox,
+                                                  unsigned long long* bar, bool part, const int base[3], int lane) {
+    WarpBox B;
+    B.lo0 = __reduce_min_sync(0xffffffffu, part ? base[0] : INT_MAX);
+    B.lo1 = __reduce_min_sync(0xffffffffu, part ? base[1] : INT_MAX);
+    B.lo2 = __reduce_min_sync(0xffffffffu, part ? base[2] : INT_MAX);
+    const int hi0 = __reduce_max_sync(0xffffffffu, part ? base[0] : INT_MIN);
+    const int hi1 = __reduce_max_sync(0xffffffffu, part ? base[1] : INT_MIN);
+    const int hi2 = __reduce_max_sync(0xffffffffu, part ? base[2] : INT_MIN);
+    B.any = B.lo0 <= hi0;
+    B.ex = hi0 - B.lo0 + 3;
+    B.ey = hi1 - B.lo1 + 3;
+    B.ez = hi2 - B.lo2 + 3;
+    B.tma = B.any && B.ex <= kTmaBoxX && B.ey <= kTmaBoxY && B.ez <= kTmaBoxZ;
+    if (B.tma && lane == 0) {
+        mbar_init_one(bar);
+        mbar_expect_tx(bar, kTmaBoxBytes);
+        tma_load_box(vbox, map, B.lo2, B.lo1, B.lo0 + P.halo, bar);
+    }
+    return B;
+}
+
+// Gather from the warp's box: the TMA copy issued by warp_box_issue when it
+// fit, else the warp's own coalesced loads (boxes up to VCAP nodes), else the
+// grid through L1. A copy that does not complete within the bounded wait
+// raises MPM_ERR_COPY_TIMEOUT, is waited for once more, and the warp gathers
+// through L1. Called by the whole warp.
+template <int VCAP>
+__device__ __forceinline__ void g2p_gather_tma(const DevParams& P, const WarpBox& B, const float4* __restrict__ vel,
+                                               float4* __restrict__ vbox, unsigned long long* bar, bool part,
+                                               bool active, const int base[3], const float fx[3], float v[3],
+                                               float C[3][3], int lane, WxSlot wx, int* err) {
+    const int lo0 = B.lo0, lo1 = B.lo1, lo2 = B.lo2;
+    int ey = B.ey, ez = B.ez;
+    bool staged = false;
+    if (B.tma) {
+        __syncwarp();
+        staged = mbar_wait_bounded(bar, 0);
+        if (!staged) {
+            if (lane == 0) raise_error(err, MPM_ERR_COPY_TIMEOUT);
+            mbar_wait_bounded(bar, 0);   // let the copy in flight land before the slice is left
+        }
+        ey = kTmaBoxY;
+        ez = kTmaBoxZ;
+    } else if (B.any && (long long)B.ex * ey * ez <= VCAP) {
+        const int vol = B.ex * ey * ez;
+        const int slab = (int)P.slab, gz = P.Gz;
+        const int g0 = ((lo0 + P.halo) * P.Gy + lo1) * gz + lo2;
+        const float inv_ez = 1.0f / (float)ez, inv_ey = 1.0f / (float)ey;
+        for (int k = lane; k < vol; k += 32) {
+            const int row = (int)(((float)k + 0.5f) * inv_ez);   // k / ez (k, ez <= VCAP)
+            const int tz = k - row * ez;
+            const int tx = (int)(((float)row + 0.5f) * inv_ey);
+            const int ty = row - tx * ey;
+            vbox[k] = __ldg(vel + (g0 + tx * slab + ty * gz + tz));
+        }
+        __syncwarp();
+        staged = true;
+    }
+    if (part && staged) {
+        // v = sum w nv and the first moments M_k = sum w nv o_k over the node
+        // offsets o = (a, b, c); C = 4/h sum w nv (o - f) = 4/h (M - f v)
+        float ww[3][3];
+        quad_weights<float>(fx, ww);
+        wx.put(ww);
+        float Mx[3], My[3], Mz[3];
+#pragma unroll
+        for (int r = 0; r < 3; r++) { v[r] = 0.f; Mx[r] = 0.f; My[r] = 0.f; Mz[r] = 0.f; }
+        const int t0 = ((base[0] - lo0) * ey + (base[1] - lo1)) * ez + (base[2] - lo2);
+#pragma unroll 1
+        for (int a = 0; a < 3; a++) {
+            const float wa = wx.get(a);
+            float ra[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                const float wab = wa * ww[b][1];
+                const float4* row = vbox + (t0 + a * ey * ez + b * ez);
+                float rb[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const float4 nd = row[c];
+                    const float w = wab * ww[c][2];
+                    const float wn[3] = {w * nd.x, w * nd.y, w * nd.z};
+#pragma unroll
+                    for (int r = 0; r < 3; r++) {
+                        rb[r] += wn[r];
+                        if (c == 1) Mz[r] += wn[r];
+                        if (c == 2) Mz[r] += 2.0f * wn[r];
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    ra[r] += rb[r];
+                    if (b == 1) My[r] += rb[r];
+                    if (b == 2) My[r] += 2.0f * rb[r];
+                }
+            }
+            const float fa = (float)a;
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                v[r] += ra[r];
+                Mx[r] += fa * ra[r];
+            }
+        }
+        const float s4 = 4.0f * (float)P.h_inv;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            C[r][0] = s4 * (Mx[r] - fx[0] * v[r]);
+            C[r][1] = s4 * (My[r] - fx[1] * v[r]);
+            C[r][2] = s4 * (Mz[r] - fx[2] * v[r]);
+        }
+    } else if (active) {
+        g2p_gather_mixed(P, vel, base, fx, v, C, !part, wx);
+    }
+    __syncwarp();
+}
+
 // Return map of a crushed point in FP64 (mpm_kernels.cuh:486-544). Out of
 // line (it is rare and register-hungry); arguments and result travel by
 // value so that nothing of the caller is forced into local memory.
@@ -750,16 +926,19 @@ __global__ void __launch_bounds__(256) k_p2g_mixed(DevParams P, MixedState s, in
 // atomics, 2 = FP32 shared-memory tile, 3 = int32 fixed-point shared-memory
 // tile (2 and 3 fall back to 0 when the box is too big), 4 = direct float4
 // atomics with same-cell pairs merged. GATHER: 0 = from the grid through
-// L1, 1 = from the warp's velocity box staged in shared memory (dynamic
-// shared memory of 4 x kVBoxNodes float4; SCATTER 0, 1, 4 only).
+// L1, 1 = from the warp's velocity box staged in shared memory by the warp's
+// loads (dynamic shared memory of 4 x kVBoxNodes float4), 2 = the box brought
+// in by one TMA tensor copy per warp (4 x kTmaSliceNodes float4; vel_map).
 constexpr int kVBoxNodes = 256;
 template <int MINB, int SCATTER, int GATHER = 0>
 __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedState s, int n,
                                                            const float4* __restrict__ vel, float4* __restrict__ acc,
                                                            int do_p2g, int record_pq, int store_vc, int* err,
                                                            int tile_cap, int* __restrict__ rm_list,
-                                                           int* __restrict__ rm_count) {
-    extern __shared__ float mixed_tile[];
+                                                           int* __restrict__ rm_count,
+                                                           const __grid_constant__ CUtensorMap vel_map) {
+    extern __shared__ __align__(128) float mixed_tile[];
+    __shared__ unsigned long long vbox_bar[4];
     __shared__ float wx_slots[3 * 128];
     const WxSlot wx{wx_slots + threadIdx.x};
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -767,10 +946,13 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     bool active = i < n;
     int X[3] = {0, 0, 0}, st = (int)kDisabled;
     float E[3][3], Jp = 1.f;
-    if (active) load_mixed(s, i, X, E, Jp, st);
+    // positions and status first: the gather box (and its copy) depends on them
+    if (active) {
+        st = s.status[i];
+#pragma unroll
+        for (int d = 0; d < 3; d++) X[d] = s.X[d * s.pitch + i];
+    }
     active = active && !(st & (int)kDisabled);
-    const int st_in = st;
-    const float jp_in = Jp;
 
     int base[3] = {0, 0, 0};
     float fx[3] = {1.f, 1.f, 1.f}, v[3] = {0, 0, 0}, C[3][3];
@@ -783,7 +965,23 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
         e0 = stencil_error(P, base[0], base[1], base[2]);
         if (e0) raise_error(err, e0);
     }
-    if (GATHER == 1) {
+    float4* const vbox_tma = reinterpret_cast<float4*>(mixed_tile) + (threadIdx.x >> 5) * kTmaSliceNodes;
+    WarpBox wbox;
+    if (GATHER == 2)
+        wbox = warp_box_issue(P, &vel_map, vbox_tma, &vbox_bar[threadIdx.x >> 5], active && e0 == 0, base, lane);
+    if (active) {
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) E[r][c] = s.E[(3 * r + c) * s.pitch + i];
+        Jp = s.Jp[i];
+    }
+    const int st_in = st;
+    const float jp_in = Jp;
+    if (GATHER == 2) {
+        g2p_gather_tma<kTmaSliceNodes>(P, wbox, vel, vbox_tma, &vbox_bar[threadIdx.x >> 5], active && e0 == 0,
+                                       active, base, fx, v, C, lane, wx, err);
+    } else if (GATHER == 1) {
         float4* vbox = reinterpret_cast<float4*>(mixed_tile) + (threadIdx.x >> 5) * kVBoxNodes;
         g2p_gather_staged<kVBoxNodes>(P, vel, vbox, active && e0 == 0, active, base, fx, v, C, lane, wx);
     } else if (active) {

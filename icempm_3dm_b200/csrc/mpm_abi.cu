@@ -15,6 +15,8 @@
 #include <new>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include "../../include/icempm_b200.h"
@@ -83,6 +85,8 @@ struct mpm_handle {
     int mixed_variant = 3;            // fused kernel occupancy target: 3 = 8 blocks of 128 per SM (test hook)
     int mixed_scatter = 4;            // fused kernel scatter: 0 warp-reduced, 1 direct, 2/3 tiles, 4 pairs (default)
     int mixed_gather = 1;             // fused kernel gather: 0 through L1, 1 staged warp box (default)
+    CUtensorMap vel_map;              // the velocity grid as a 4-D tensor for the TMA box copies
+    bool vel_map_ok = false;
     int* rm_list = nullptr;           // crushed points deferred to k_return_map_mixed (n entries)
     int* rm_counts = nullptr;         // two list counters, used alternately by successive launches
     int rm_parity = 0;
@@ -303,6 +307,36 @@ int launch_update(mpm_handle* h, double ind_x, double ind_y, double* force3) {
     return MPM_OK;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda); null when the driver does not provide it.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// The float4 velocity grid as the 4-D FP32 tensor (component, z, y, x) with
+// the fixed gather box of the TMA path: 4 x kTmaBoxZ x kTmaBoxY x kTmaBoxX.
+bool make_vel_map(mpm_handle* h) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const DevParams& d = h->dp;
+    const cuuint64_t dims[4] = {4, (cuuint64_t)d.Gz, (cuuint64_t)d.Gy, (cuuint64_t)(d.nodes / d.slab)};
+    const cuuint64_t strides[3] = {16, 16ull * (cuuint64_t)d.Gz, 16ull * (cuuint64_t)d.slab};
+    const cuuint32_t box[4] = {4, (cuuint32_t)kTmaBoxZ, (cuuint32_t)kTmaBoxY, (cuuint32_t)kTmaBoxX};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return enc(&h->vel_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->gvel, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Return map and P2G of the crushed points the last fused launch listed
 // (one persistent grid of 4 blocks per SM walks the list).
 int launch_return_map_mixed(mpm_handle* h, int do_p2g) {
@@ -324,12 +358,27 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
     const unsigned nb = blocks_for(n, 128);
     const int sc = h->mixed_scatter;
     int* const rm_count = h->rm_counts + h->rm_parity;
+    if (h->mixed_gather == 2 && h->vel_map_ok) {
+        // TMA gather box: 4 warps x kTmaSliceNodes float4 of dynamic shared memory
+        const size_t tmsm = sizeof(float4) * 4 * kTmaSliceNodes;
+        if (sc == 4)
+            k_g2p2g_mixed<8, 4, 2><<<nb, 128, tmsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,
+                                                                 record_pq, store_vc, h->err, 0, h->rm_list, rm_count,
+                                                                 h->vel_map);
+        else
+            k_g2p2g_mixed<8, 1, 2><<<nb, 128, tmsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,
+                                                                 record_pq, store_vc, h->err, 0, h->rm_list, rm_count,
+                                                                 h->vel_map);
+        CK_LAUNCH(h, "g2p2g mixed (TMA gather)");
+        return MPM_OK;
+    }
     if (h->mixed_gather) {
         // staged gather: 4 warps x kVBoxNodes float4 of dynamic shared memory
         const size_t vsm = sizeof(float4) * 4 * kVBoxNodes;
 #define FUSED_G(MINB, SC)                                                                                           \
     k_g2p2g_mixed<MINB, SC, 1><<<nb, 128, vsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,    \
-                                                            record_pq, store_vc, h->err, 0, h->rm_list, rm_count)
+                                                            record_pq, store_vc, h->err, 0, h->rm_list, rm_count,  \
+                                                            h->vel_map)
         if (h->mixed_variant == 1) {
             if (sc == 4) FUSED_G(5, 4);
             else if (sc == 0) FUSED_G(5, 0);
@@ -350,7 +399,7 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
 #define FUSED(MINB, SC)                                                                                          \
     k_g2p2g_mixed<MINB, SC><<<nb, 128, tsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,     \
                                                          record_pq, store_vc, h->err, kMixedTileNodes, h->rm_list,  \
-                                                         rm_count)
+                                                         rm_count, h->vel_map)
 #define FUSED_SC(MINB)                  \
     if (sc == 4) FUSED(MINB, 4);        \
     else if (sc == 3) FUSED(MINB, 3);   \
@@ -581,6 +630,8 @@ mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity
                 break;
             }
             cudaMemsetAsync(h->rm_counts, 0, sizeof(int) * 2, h->stream);
+            std::memset(&h->vel_map, 0, sizeof(h->vel_map));
+            h->vel_map_ok = make_vel_map(h);
             cudaMemsetAsync(h->mx, 0, sizeof(float) * MPM_N_PTS_ARRAYS * h->pitch, h->stream);
             cudaMemsetAsync(h->gacc, 0, sizeof(float4) * (size_t)h->dp.nodes, h->stream);
             cudaMemsetAsync(h->gvel, 0, sizeof(float4) * (size_t)h->dp.nodes, h->stream);
@@ -982,11 +1033,12 @@ int mpm_testing_active_nodes(mpm_handle* h, long long* count) {
 }
 
 int mpm_testing_set_g2p_variant(mpm_handle* h, int variant) {
-    if (!h || variant < 0 || variant > 5) return MPM_ERR_ARG;
+    if (!h || variant < 0 || variant > 6) return MPM_ERR_ARG;
     if (variant >= 3) {
         if (!is_mixed(h)) return MPM_ERR_ARG;
+        if (variant == 6 && !h->vel_map_ok) return MPM_ERR_ARG;
         h->mixed_variant = variant == 3 ? 2 : variant == 4 ? 1 : 3;
-        h->mixed_gather = 1;
+        h->mixed_gather = variant == 6 ? 2 : 1;
         return MPM_OK;
     }
     h->g2p_variant = variant;

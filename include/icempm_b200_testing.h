@@ -27,7 +27,9 @@ int mpm_testing_set_p2g_variant(mpm_handle* h, int variant);
  * SM, 1 = 3 blocks, 2 = 6 blocks (default; fewer registers per thread). In
  * the mixed mode the fused kernel's target: 0 = 4, 1 = 5, 2 = 6 blocks;
  * 3 = 6, 4 = 5 and 5 = 8 blocks (default) with each warp's velocity box
- * staged in shared memory for the gather (mixed mode only). */
+ * staged in shared memory for the gather by the warp's loads, 6 = 8 blocks
+ * with the box brought in by one TMA tensor copy per warp (mixed mode only;
+ * MPM_ERR_ARG where the driver cannot encode the tensor map). */
 int mpm_testing_set_g2p_variant(mpm_handle* h, int variant);
 
 /* Runs the device 3x3 SVD on `count` row-major matrices A (9 doubles each)
