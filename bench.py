@@ -11,8 +11,8 @@ lattice. One "step" is one substep of Model3D::Step on the whole block.
 value: particle-steps/s over all ranks with the state resident on the device
 (timed with CUDA events on the handle's stream, barrier + synchronize on both
 sides, max over ranks). e2e: the same metric through the public C-ABI with
-host buffers (pinned SoA uploaded, K substeps with the force history read
-back, SoA downloaded) inside the timed region. N > 1 runs independent
+host buffers (pinned SoA and cohesion uploaded, the cell-key sort, K substeps
+with the force history read back, SoA downloaded) inside the timed region. N > 1 runs independent
 replicas, one per GPU (the path is one partition; no collective).
 
 --impl reference times the CPU port of the reference step (the oracle,
@@ -291,6 +291,7 @@ def run_ours(args):
     h2 = MPMHandle(prms, n, prec, device=local)
     h2.set_stream(stream.cuda_stream)
     h2.upload(host_np, cohesion=coh)
+    h2.sort()
     h2.step(3, want_forces=False)
     if dist is not None:
         dist.barrier()
@@ -299,6 +300,7 @@ def run_ours(args):
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     h2.upload(host_np, cohesion=coh)
+    h2.sort()                    # cell order, as the reference's RemoveDisabledAndSort
     h2.step(args.steps)
     from icempm_3dm_b200._lib import LIB, dptr
     import ctypes
@@ -311,7 +313,8 @@ def run_ours(args):
     soa_bytes = soa.nbytes + (coh.nbytes if coh is not None else 0)
     e2e = {"value": world * n * args.steps / (e2e_ms * 1e-3), "unit": "particle-steps/s",
            "h2d_bytes_per_step": soa_bytes / args.steps,
-           "d2h_bytes_per_step": (soa.nbytes + 24 * args.steps) / args.steps}
+           "d2h_bytes_per_step": (soa.nbytes + 24 * args.steps) / args.steps,
+           "calls": "mpm_upload_soa + mpm_upload_cohesion + mpm_sort + mpm_step(K) + mpm_download_soa"}
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

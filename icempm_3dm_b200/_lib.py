@@ -140,6 +140,7 @@ ENTRY_POINTS = [
     ("mpm_testing_sizeof_params", ctypes.c_size_t, []),
     ("mpm_testing_step_timed", ctypes.c_int, [_hp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
     ("mpm_testing_active_nodes", ctypes.c_int, [_hp, ctypes.POINTER(ctypes.c_longlong)]),
+    ("mpm_testing_copy_wait_timeout", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     ("mpm_testing_download_grid", ctypes.c_int, [_hp, _dp, ctypes.c_int]),
 ]
 

@@ -31,7 +31,28 @@ struct DevParams {
     double drag;
     // failure-surface constants for GrainVariability = 0 (FP32 fast path)
     float fs_pmin2, fs_k, fs_msq, fs_1p2b, fs_bpmax, fs_pmax;
+    double inv_gz, inv_gy;         // 1 / Gz, 1 / Gy for node index -> (x, y, z)
 };
+
+// q = n / d and r = n % d for 0 <= n < 2^31 with the double reciprocal of d:
+// the product is within 2^-22 of n/d, so one correction step makes it exact.
+__device__ __forceinline__ long long div_by64(long long n, int d, double inv_d, int& r) {
+    // as div_by for 0 <= n < 2^50: the quotient estimate is off by at most 1
+    long long q = (long long)((double)n * inv_d);
+    long long rr = n - q * d;
+    if (rr < 0) { q--; rr += d; }
+    else if (rr >= d) { q++; rr -= d; }
+    r = (int)rr;
+    return q;
+}
+
+__device__ __forceinline__ int div_by(int n, int d, double inv_d, int& r) {
+    int q = __double2int_rz((double)n * inv_d);
+    r = n - q * d;
+    if (r < 0) { q--; r += d; }
+    else if (r >= d) { q++; r -= d; }
+    return q;
+}
 
 constexpr double kCoeff1 = 1.224744871391589;      // sqrt(3/2)
 constexpr double kCoeff1Inv = 0.8164965809277260;  // 1/sqrt(3/2)

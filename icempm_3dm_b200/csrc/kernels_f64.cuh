@@ -436,9 +436,9 @@ __global__ void __launch_bounds__(BLOCK) k_update_f64(DevParams P, double* __res
         const double mass = grid[idx];
         if (mass != 0) {
             double v[3] = {grid[P.gstride + idx], grid[2 * P.gstride + idx], grid[3 * P.gstride + idx]};
-            const int idx_z = (int)(idx % P.Gz);
-            const int idx_y = (int)((idx / P.Gz) % P.Gy);
-            const int idx_x = (int)(idx / P.slab);
+            int idx_z, idx_y;
+            const long long col = div_by64(idx, P.Gz, P.inv_gz, idx_z);
+            const int idx_x = (int)div_by64(col, P.Gy, P.inv_gy, idx_y);
             const int gx = idx_x - P.halo, gy = idx_y, gz = idx_z;
 #pragma unroll
             for (int k = 0; k < 3; k++) v[k] /= mass;

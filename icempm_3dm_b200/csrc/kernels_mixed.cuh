@@ -350,11 +350,26 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
     return ok != 0;
 }
 
-// Bounded wait for phase `parity` of bar: false when kTmaWaitPolls polls passed.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-    for (int k = 0; k < kTmaWaitPolls; k++)
+// Bounded wait for phase `parity` of bar: false when `polls` polls passed.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
+                                                  int polls = kTmaWaitPolls) {
+    for (int k = 0; k < polls; k++)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
+}
+
+// Test of the bounded wait's error path: one warp arms an mbarrier for 16
+// bytes that no copy delivers (nothing is in flight), waits at most `polls`
+// polls and records MPM_ERR_COPY_TIMEOUT, or 0 if the phase completed.
+__global__ void k_wait_timeout_probe(int polls, int* status) {
+    __shared__ unsigned long long bar;
+    if (threadIdx.x == 0) {
+        mbar_init_one(&bar);
+        mbar_expect_tx(&bar, 16u);
+    }
+    __syncwarp();
+    const bool done = mbar_wait_bounded(&bar, 0, polls);
+    if (threadIdx.x == 0) *status = done ? 0 : MPM_ERR_COPY_TIMEOUT;
 }
 
 __device__ __forceinline__ void tma_load_box(void* dst, const CUtensorMap* map, int z0, int y0, int x0,
@@ -1146,27 +1161,27 @@ __global__ void __launch_bounds__(128) k_return_map_mixed(DevParams P, MixedStat
     }
 }
 
-// Node update for the mixed grid: FP64 arithmetic on the FP32 sums, contact
-// force in FP64 (sensor and per-substep total), velocities written as float4,
-// the accumulator cleared for the next P2G.
+// Node update for the mixed grid: FP64 arithmetic on the FP32 sums (one
+// reciprocal of the mass), contact force in FP64 (sensor and per-substep
+// total), velocities written as float4, the accumulator cleared for the next
+// P2G. Node coordinates by reciprocal multiplication (no integer division).
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_update_mixed(DevParams P, float4* __restrict__ acc, float4* __restrict__ vel,
                                                         double ind_x, double ind_y, double* __restrict__ sensor,
                                                         double* __restrict__ force3) {
-    const long long idx = (long long)blockIdx.x * BLOCK + threadIdx.x;
+    const int idx = blockIdx.x * BLOCK + threadIdx.x;   // the handle keeps nodes < 2^31
     double f[3] = {0, 0, 0};
     if (idx < P.nodes) {
         const float4 a = acc[idx];
         const double mass = a.x;
         if (mass != 0) {
             acc[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
-            double v[3] = {(double)a.y, (double)a.z, (double)a.w};
-            const int idx_z = (int)(idx % P.Gz);
-            const int idx_y = (int)((idx / P.Gz) % P.Gy);
-            const int idx_x = (int)(idx / P.slab);
+            int idx_z, idx_y;
+            const int col = div_by(idx, P.Gz, P.inv_gz, idx_z);
+            const int idx_x = div_by(col, P.Gy, P.inv_gy, idx_y);
             const int gx = idx_x - P.halo, gy = idx_y, gz = idx_z;
-#pragma unroll
-            for (int k = 0; k < 3; k++) v[k] /= mass;
+            const double inv_m = 1.0 / mass;
+            double v[3] = {(double)a.y * inv_m, (double)a.z * inv_m, (double)a.w * inv_m};
             v[1] -= P.dt_gravity;
             const double vsq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
             if (vsq > P.vmax_sq) {

@@ -34,6 +34,19 @@ __global__ void k_narrow(const double* __restrict__ src, float* __restrict__ dst
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = (float)src[i];
 }
+// p0 = c / tan(phi) in place (and its FP32 copy for the mixed state)
+__global__ void k_cohesion_to_apex(double* __restrict__ p0, float* __restrict__ p0f, int n, double tan_phi) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = p0[i] / tan_phi;
+    p0[i] = v;
+    if (p0f) p0f[i] = (float)v;
+}
+// ids = 0, 1, ..., n-1 (the upload order)
+__global__ void k_iota(unsigned* __restrict__ ids, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) ids[i] = (unsigned)i;
+}
 constexpr int kMixedTileNodes = 2048;   // 32 KB FP32 tile of the fused mixed kernel
 constexpr int kFxBlock = 256;   // threads of the fixed-point P2G
 constexpr int kFxPPT = 4;       // particles per thread (1024-particle chunks)
@@ -144,6 +157,8 @@ DevParams make_dev_params(const SimParams3D& p) {
     d.setup_type = p.SetupType;
     d.subdiv = p.IndenterSubdivisions;
     d.slab = (long long)p.GridY * p.GridZ;
+    d.inv_gz = 1.0 / (double)p.GridZ;
+    d.inv_gy = 1.0 / (double)p.GridY;
     d.nodes = (long long)(p.GridXTotal + 2 * p.GridHaloSize) * d.slab;
     d.gstride = (d.nodes + 31) / 32 * 32;
     d.h = p.cellsize;
@@ -684,10 +699,9 @@ int mpm_upload_soa(mpm_handle* h, const double* soa, unsigned pitch, unsigned n)
     if (n) {
         CK(h, cudaMemcpy2DAsync(h->pts, sizeof(double) * h->pitch, soa, sizeof(double) * pitch, sizeof(double) * n,
                                 MPM_N_PTS_ARRAYS, cudaMemcpyHostToDevice, h->stream));
-        std::vector<unsigned> ids(n);
-        for (unsigned i = 0; i < n; i++) ids[i] = i;
-        CK(h, cudaMemcpyAsync(h->ids, ids.data(), sizeof(unsigned) * n, cudaMemcpyHostToDevice, h->stream));
-        CK(h, cudaStreamSynchronize(h->stream));
+        k_iota<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->ids, (int)n);
+        CK_LAUNCH(h, "ids");
+        CK(h, cudaStreamSynchronize(h->stream));   // soa may be released when the call returns
     }
     h->n = n;
     h->uploaded = true;
@@ -714,16 +728,16 @@ int mpm_upload_cohesion(mpm_handle* h, const double* c, unsigned n) {
     }
     if (n != h->n || h->prms.DP_tan_phi == 0) return MPM_ERR_ARG;
     if (!h->p0) CK(h, cudaMalloc(&h->p0, sizeof(double) * h->pitch));
-    std::vector<double> p0(n);
-    for (unsigned i = 0; i < n; i++) p0[i] = c[i] / h->prms.DP_tan_phi;
-    CK(h, cudaMemcpyAsync(h->p0, p0.data(), sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
-    CK(h, cudaStreamSynchronize(h->stream));
+    if (is_mixed(h) && !h->p0f) CK(h, cudaMalloc(&h->p0f, sizeof(float) * h->pitch));
     h->p2g_ready = false;
-    if (is_mixed(h) && n) {
-        if (!h->p0f) CK(h, cudaMalloc(&h->p0f, sizeof(float) * h->pitch));
-        k_narrow<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->p0, h->p0f, (int)n);
-        CK_LAUNCH(h, "p0 narrow");
-    }
+    if (n == 0) return MPM_OK;
+    // cohesion to the device as given, then p0 = c / tan(phi) there (the same
+    // correctly rounded FP64 division as on the host)
+    CK(h, cudaMemcpyAsync(h->p0, c, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    k_cohesion_to_apex<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->p0, is_mixed(h) ? h->p0f : nullptr, (int)n,
+                                                                  h->prms.DP_tan_phi);
+    CK_LAUNCH(h, "cohesion to apex shift");
+    CK(h, cudaStreamSynchronize(h->stream));   // c may be released when the call returns
     return MPM_OK;
 }
 
@@ -1011,6 +1025,19 @@ int mpm_testing_step_timed(mpm_handle* h, int nsteps, float* ms) {
     }
     for (int k = 0; k < 6; k++) cudaEventDestroy(ev[k]);
     return r;
+}
+
+int mpm_testing_copy_wait_timeout(int device, int polls, int* status) {
+    if (!status || polls <= 0) return MPM_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return MPM_ERR_NO_DEVICE;
+    int* d = nullptr;
+    if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return MPM_ERR_CUDA;
+    cudaMemset(d, 0xff, sizeof(int));
+    k_wait_timeout_probe<<<1, 32>>>(polls, d);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(status, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
 }
 
 int mpm_testing_active_nodes(mpm_handle* h, long long* count) {

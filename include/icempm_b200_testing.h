@@ -52,6 +52,12 @@ int mpm_testing_download_grid(mpm_handle* h, double* out, int which);
  * G2P->P2G] (mixed mode). */
 int mpm_testing_step_timed(mpm_handle* h, int nsteps, float* ms);
 
+/* The bounded wait of the kernels' asynchronous (TMA) copies, run on an
+ * mbarrier armed for bytes that no copy delivers (nothing is in flight):
+ * *status receives MPM_ERR_COPY_TIMEOUT after `polls` polls (0 would mean the
+ * phase completed). Returns 0, or MPM_ERR_CUDA if the launch failed. */
+int mpm_testing_copy_wait_timeout(int device, int polls, int* status);
+
 /* Number of grid nodes with non-zero mass in the current P2G result (the
  * accumulator in mixed mode; the grid after P2G in FP64 modes). */
 int mpm_testing_active_nodes(mpm_handle* h, long long* count);

@@ -205,3 +205,18 @@ def test_out_of_grid_error_codes(axis, side, code):
         r = h.step(1, raise_on_error=False, want_forces=False)
         assert r == code
         assert h.error() == code
+
+
+def test_bounded_copy_wait_reports_timeout_and_context_stays_usable():
+    """The kernels' wait on an asynchronous copy gives up after its poll limit
+    with MPM_ERR_COPY_TIMEOUT (here on an mbarrier that no copy feeds; nothing
+    is in flight), and the context keeps working."""
+    import ctypes
+    st = ctypes.c_int(-1)
+    check(LIB.mpm_testing_copy_wait_timeout(0, 1000, ctypes.byref(st)), "copy wait probe")
+    assert st.value == 110
+    prms, soa = perturbed_block(n=500, seed=3)
+    with MPMHandle(prms, soa.shape[1]) as h:
+        h.upload(soa)
+        hist = h.step(2)
+    assert np.all(np.isfinite(hist))
