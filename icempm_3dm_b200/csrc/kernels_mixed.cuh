@@ -387,10 +387,17 @@ __device__ __forceinline__ void tma_load_box(void* dst, const CUtensorMap* map, 
 // 0 as soon as the bases are known, so that it overlaps the particles' other
 // loads). Called by the whole warp.
 struct WarpBox {
-    int lo0, lo1, lo2, ex, ey, ez;
-    bool any, tma;
+    int lo0, lo1, lo2;
+    int dims;   // ex | ey << 8 | ez << 16 | any << 24 | tma << 25 (extents <= 255 when used)
+    __device__ __forceinline__ int ex() const { return dims & 255; }
+    __device__ __forceinline__ int ey() const { return (dims >> 8) & 255; }
+    __device__ __forceinline__ int ez() const { return (dims >> 16) & 255; }
+    __device__ __forceinline__ bool any() const { return (dims >> 24) & 1; }
+    __device__ __forceinline__ bool tma() const { return (dims >> 25) & 1; }
 };
 
+// Computes the box and, when it fits, initialises the warp's mbarrier (one
+// use per launch) and issues the tensor copy (lane 0).
 __device__ __forceinline__ WarpBox warp_box_issue(const DevParams& P, const CUtensorMap* map, float4* vbox,
                                                   unsigned long long* bar, bool part, const int base[3], int lane) {
     WarpBox B;
@@ -400,12 +407,12 @@ __device__ __forceinline__ WarpBox warp_box_issue(const DevParams& P, const CUte
     const int hi0 = __reduce_max_sync(0xffffffffu, part ? base[0] : INT_MIN);
     const int hi1 = __reduce_max_sync(0xffffffffu, part ? base[1] : INT_MIN);
     const int hi2 = __reduce_max_sync(0xffffffffu, part ? base[2] : INT_MIN);
-    B.any = B.lo0 <= hi0;
-    B.ex = hi0 - B.lo0 + 3;
-    B.ey = hi1 - B.lo1 + 3;
-    B.ez = hi2 - B.lo2 + 3;
-    B.tma = B.any && B.ex <= kTmaBoxX && B.ey <= kTmaBoxY && B.ez <= kTmaBoxZ;
-    if (B.tma && lane == 0) {
+    const bool any = B.lo0 <= hi0;
+    const int ex = any ? hi0 - B.lo0 + 3 : 0, ey = any ? hi1 - B.lo1 + 3 : 0, ez = any ? hi2 - B.lo2 + 3 : 0;
+    const bool tma = any && ex <= kTmaBoxX && ey <= kTmaBoxY && ez <= kTmaBoxZ;
+    const bool small = any && ex <= 255 && ey <= 255 && ez <= 255;
+    B.dims = small ? (ex | (ey << 8) | (ez << 16) | (1 << 24) | ((int)tma << 25)) : 0;
+    if (tma && lane == 0) {
         mbar_init_one(bar);
         mbar_expect_tx(bar, kTmaBoxBytes);
         tma_load_box(vbox, map, B.lo2, B.lo1, B.lo0 + P.halo, bar);
@@ -424,9 +431,9 @@ __device__ __forceinline__ void g2p_gather_tma(const DevParams& P, const WarpBox
                                                bool active, const int base[3], const float fx[3], float v[3],
                                                float C[3][3], int lane, WxSlot wx, int* err) {
     const int lo0 = B.lo0, lo1 = B.lo1, lo2 = B.lo2;
-    int ey = B.ey, ez = B.ez;
+    int ey = B.ey(), ez = B.ez();
     bool staged = false;
-    if (B.tma) {
+    if (B.tma()) {
         __syncwarp();
         staged = mbar_wait_bounded(bar, 0);
         if (!staged) {
@@ -435,8 +442,8 @@ __device__ __forceinline__ void g2p_gather_tma(const DevParams& P, const WarpBox
         }
         ey = kTmaBoxY;
         ez = kTmaBoxZ;
-    } else if (B.any && (long long)B.ex * ey * ez <= VCAP) {
-        const int vol = B.ex * ey * ez;
+    } else if (B.any() && B.ex() * ey * ez <= VCAP) {
+        const int vol = B.ex() * ey * ez;
         const int slab = (int)P.slab, gz = P.Gz;
         const int g0 = ((lo0 + P.halo) * P.Gy + lo1) * gz + lo2;
         const float inv_ez = 1.0f / (float)ez, inv_ey = 1.0f / (float)ey;
@@ -936,6 +943,123 @@ __global__ void __launch_bounds__(256) k_p2g_mixed(DevParams P, MixedState s, in
     p2g_scatter_mixed(P, acc, active, inside, base, fx, mass, mv, S, lane);
 }
 
+// G2P tail of the fused kernels for one particle (whole warp): fixed-point
+// advection, E <- E + dt C (I + E), trial p and q, the failure test, the P/Q
+// record; a newly crushed point is appended to rm_list (its return map and
+// P2G run in k_return_map_mixed) and returns true. Stores X and E; v and C
+// only when store_vc or crushed (the next G2P recomputes them from the grid);
+// Jp_inv and status only when they changed.
+__device__ __forceinline__ bool fused_update_state(const DevParams& P, const MixedState& s, int i, bool active,
+                                                   int X[3], int& st, int st_in, float jp_in, float E[3][3],
+                                                   float& Jp, const float v[3], const float C[3][3],
+                                                   ElasticInv& inv, int record_pq, int store_vc,
+                                                   int* __restrict__ rm_list, int* __restrict__ rm_count, int lane) {
+    bool need_rm = false;
+    if (active) {
+        const float dt = (float)P.dt;
+        const float adv = dt * (float)P.h_inv * kFixScale;
+#pragma unroll
+        for (int d = 0; d < 3; d++) X[d] += __float2int_rn(v[d] * adv);
+        float En[3][3];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                En[r][c] = E[r][c] + dt * (C[r][c] + (C[r][0] * E[0][c] + C[r][1] * E[1][c] + C[r][2] * E[2][c]));
+        float p_tr = 0.f, q_tr = 0.f;
+        if (st & (int)kLiquid) {
+            float A[3][3];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) A[r][c] = dt * C[r][c];
+            Jp *= 1.0f + detm1(A);
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) E[r][c] = En[r][c];
+        } else {
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) E[r][c] = En[r][c];
+            inv = elastic_invariants(E);
+            trial_pq_inv(P, inv, p_tr, q_tr);
+            if (!(st & (int)kCrushed) && outside_failure_surface_f32(P, (short)st, p_tr, q_tr)) st |= (int)kCrushed;
+            need_rm = (st & (int)kCrushed) != 0;
+        }
+        if (record_pq) {
+            s.PQ[i] = p_tr;
+            s.PQ[s.pitch + i] = q_tr;
+        }
+    }
+    const unsigned rm_mask = __ballot_sync(0xffffffffu, need_rm);
+    if (rm_mask) {
+        const int first = __ffs(rm_mask) - 1;
+        int slot0 = 0;
+        if (lane == first) slot0 = atomicAdd(rm_count, __popc(rm_mask));
+        slot0 = __shfl_sync(0xffffffffu, slot0, first);
+        if (need_rm) rm_list[slot0 + __popc(rm_mask & ((1u << lane) - 1u))] = i;
+    }
+    if (active) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) s.X[d * s.pitch + i] = X[d];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) s.E[(3 * r + c) * s.pitch + i] = E[r][c];
+        if (store_vc || need_rm) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) s.v[d * s.pitch + i] = v[d];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) s.C[(3 * r + c) * s.pitch + i] = C[r][c];
+        }
+        if (__float_as_int(Jp) != __float_as_int(jp_in)) s.Jp[i] = Jp;
+        if (st != st_in) s.status[i] = st;
+    }
+    return need_rm;
+}
+
+// P2G payload of the fused kernels (S = m C - dt V Dp^-1 tau, mpm_kernels.cuh:63)
+// at the advected position; inactive lanes get a zero payload.
+__device__ __forceinline__ void fused_payload(const DevParams& P, bool active, const int X[3], int st,
+                                              const float E[3][3], const float C[3][3], const float v[3], float Jp,
+                                              const ElasticInv& inv, int base[3], float fx[3], float& mass,
+                                              float mv[3], float S[3][3], bool& inside, int* err) {
+    mass = 0.f;
+    inside = false;
+    if (active) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) fix_base(X[d], base[d], fx[d]);
+        if (st & (int)kLiquid) {
+            p2g_payload_mixed(P, E, C, v, true, Jp, mass, mv, S);
+        } else {
+            mass = (float)P.particle_mass;
+            float tau[3][3];
+            tau_inv(P, inv, tau);
+            const float dvd = (float)P.dt_vol_Dpinv;
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                mv[r] = v[r] * mass;
+#pragma unroll
+                for (int c = 0; c < 3; c++) S[r][c] = mass * C[r][c] - dvd * tau[r][c];
+            }
+        }
+        const int e = stencil_error(P, base[0], base[1], base[2]);
+        if (e) raise_error(err, e);
+        inside = e == 0;
+    } else {
+#pragma unroll
+        for (int d = 0; d < 3; d++) { base[d] = 0; fx[d] = 1.0f; mv[d] = 0.f; }
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) S[r][c] = 0.f;
+    }
+}
+
 // Fused G2P (this step) -> P2G (next step). do_p2g = 0 gives a plain G2P.
 // SCATTER: 0 = warp-reduced direct float4 atomics, 1 = direct float4
 // atomics, 2 = FP32 shared-memory tile, 3 = int32 fixed-point shared-memory
@@ -1002,112 +1126,12 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     } else if (active) {
         g2p_gather_mixed(P, vel, base, fx, v, C, e0 != 0, wx);
     }
-    bool need_rm = false;
-    if (active) {
-        // advection in fixed point, F <- (I + dt C) F as E <- E + dt C (I + E)
-        const float dt = (float)P.dt;
-        const float adv = dt * (float)P.h_inv * kFixScale;
-#pragma unroll
-        for (int d = 0; d < 3; d++) X[d] += __float2int_rn(v[d] * adv);
-        float En[3][3];
-#pragma unroll
-        for (int r = 0; r < 3; r++)
-#pragma unroll
-            for (int c = 0; c < 3; c++)
-                En[r][c] = E[r][c] + dt * (C[r][c] + (C[r][0] * E[0][c] + C[r][1] * E[1][c] + C[r][2] * E[2][c]));
-        float p_tr = 0.f, q_tr = 0.f;
-        if (st & (int)kLiquid) {
-            float A[3][3];
-#pragma unroll
-            for (int r = 0; r < 3; r++)
-#pragma unroll
-                for (int c = 0; c < 3; c++) A[r][c] = dt * C[r][c];
-            Jp *= 1.0f + detm1(A);
-#pragma unroll
-            for (int r = 0; r < 3; r++)
-#pragma unroll
-                for (int c = 0; c < 3; c++) E[r][c] = En[r][c];
-        } else {
-#pragma unroll
-            for (int r = 0; r < 3; r++)
-#pragma unroll
-                for (int c = 0; c < 3; c++) E[r][c] = En[r][c];
-            inv = elastic_invariants(E);
-            trial_pq_inv(P, inv, p_tr, q_tr);
-            if (!(st & (int)kCrushed) && outside_failure_surface_f32(P, (short)st, p_tr, q_tr)) st |= (int)kCrushed;
-            need_rm = (st & (int)kCrushed) != 0;
-        }
-        if (record_pq) {
-            s.PQ[i] = p_tr;
-            s.PQ[s.pitch + i] = q_tr;
-        }
-    }
-    // Crushed points leave the fused path here: their trial state is stored
-    // (v and C included) and their index appended to rm_list; the return map
-    // and their P2G run in k_return_map_mixed. No call in this kernel keeps
-    // its register allocation free of the call's save/restore traffic.
-    const unsigned rm_mask = __ballot_sync(0xffffffffu, need_rm);
-    if (rm_mask) {
-        const int first = __ffs(rm_mask) - 1;
-        int slot0 = 0;
-        if (lane == first) slot0 = atomicAdd(rm_count, __popc(rm_mask));
-        slot0 = __shfl_sync(0xffffffffu, slot0, first);
-        if (need_rm) rm_list[slot0 + __popc(rm_mask & ((1u << lane) - 1u))] = i;
-    }
-    if (active) {
-        // store state. v and C are recomputed from the grid by the next G2P
-        // and this launch's P2G takes them from registers, so they are
-        // written only when a reader follows (store_vc: download, sort, the
-        // standalone P2G, the return-map kernel); Jp_inv and the status word
-        // only when they change.
-#pragma unroll
-        for (int d = 0; d < 3; d++) s.X[d * s.pitch + i] = X[d];
-#pragma unroll
-        for (int r = 0; r < 3; r++)
-#pragma unroll
-            for (int c = 0; c < 3; c++) s.E[(3 * r + c) * s.pitch + i] = E[r][c];
-        if (store_vc || need_rm) {
-#pragma unroll
-            for (int d = 0; d < 3; d++) s.v[d * s.pitch + i] = v[d];
-#pragma unroll
-            for (int r = 0; r < 3; r++)
-#pragma unroll
-                for (int c = 0; c < 3; c++) s.C[(3 * r + c) * s.pitch + i] = C[r][c];
-        }
-        if (__float_as_int(Jp) != __float_as_int(jp_in)) s.Jp[i] = Jp;
-        if (st != st_in) s.status[i] = st;
-    }
+    const bool need_rm = fused_update_state(P, s, i, active, X, st, st_in, jp_in, E, Jp, v, C, inv, record_pq,
+                                            store_vc, rm_list, rm_count, lane);
     active = active && !need_rm;   // crushed points scatter in k_return_map_mixed
     if (!do_p2g) return;   // uniform across the launch
-    float mass = 0.f, mv[3] = {0, 0, 0}, S[3][3];
-    if (active) {
-#pragma unroll
-        for (int d = 0; d < 3; d++) fix_base(X[d], base[d], fx[d]);
-        if (st & (int)kLiquid) {
-            p2g_payload_mixed(P, E, C, v, true, Jp, mass, mv, S);
-        } else {
-            mass = (float)P.particle_mass;
-            float tau[3][3];
-            tau_inv(P, inv, tau);
-            const float dvd = (float)P.dt_vol_Dpinv;
-#pragma unroll
-            for (int r = 0; r < 3; r++) {
-                mv[r] = v[r] * mass;
-#pragma unroll
-                for (int c = 0; c < 3; c++) S[r][c] = mass * C[r][c] - dvd * tau[r][c];
-            }
-        }
-        const int e = stencil_error(P, base[0], base[1], base[2]);
-        if (e) raise_error(err, e);
-        inside = e == 0;
-    } else {
-#pragma unroll
-        for (int d = 0; d < 3; d++) { base[d] = 0; fx[d] = 1.0f; }
-#pragma unroll
-        for (int r = 0; r < 3; r++)
-#pragma unroll
-            for (int c = 0; c < 3; c++) S[r][c] = 0.f;
-    }
+    float mass, mv[3], S[3][3];
+    fused_payload(P, active, X, st, E, C, v, Jp, inv, base, fx, mass, mv, S, inside, err);
     if (SCATTER == 2 && p2g_scatter_tile<128>(P, acc, mixed_tile, tile_cap, active, inside, base, fx, mass, mv, S, lane))
         return;
     if (SCATTER == 3 && p2g_scatter_tile_fx<128>(P, acc, reinterpret_cast<int*>(mixed_tile), tile_cap, active, inside,

@@ -98,6 +98,7 @@ struct mpm_handle {
     int mixed_variant = 3;            // fused kernel occupancy target: 3 = 8 blocks of 128 per SM (test hook)
     int mixed_scatter = 4;            // fused kernel scatter: 0 warp-reduced, 1 direct, 2/3 tiles, 4 pairs (default)
     int mixed_gather = 1;             // fused kernel gather: 0 through L1, 1 staged warp box (default)
+    int num_sms = 148;
     CUtensorMap vel_map;              // the velocity grid as a 4-D tensor for the TMA box copies
     bool vel_map_ok = false;
     int* rm_list = nullptr;           // crushed points deferred to k_return_map_mixed (n entries)
@@ -357,8 +358,8 @@ bool make_vel_map(mpm_handle* h) {
 int launch_return_map_mixed(mpm_handle* h, int do_p2g) {
     const int cur = h->rm_parity;
     h->rm_parity ^= 1;
-    k_return_map_mixed<<<148 * 4, 128, 0, h->stream>>>(h->dp, mixed_state(h), h->rm_list, h->rm_counts + cur,
-                                                       h->rm_counts + (cur ^ 1), h->gacc, do_p2g, h->err);
+    k_return_map_mixed<<<h->num_sms * 4, 128, 0, h->stream>>>(h->dp, mixed_state(h), h->rm_list, h->rm_counts + cur,
+                                                              h->rm_counts + (cur ^ 1), h->gacc, do_p2g, h->err);
     CK_LAUNCH(h, "return map mixed");
     return MPM_OK;
 }
@@ -612,6 +613,7 @@ mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity
         h->precision = precision;
         h->device = device;
         h->capacity = capacity;
+        h->num_sms = prop.multiProcessorCount;
         h->pitch = ((size_t)capacity + 31) / 32 * 32;
         if (cudaSetDevice(device) != cudaSuccess) { st = MPM_ERR_CUDA; break; }
         if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) { st = MPM_ERR_CUDA; break; }
