@@ -132,6 +132,7 @@ ENTRY_POINTS = [
     ("mpm_adjoint_forward", ctypes.c_int, [_hp, ctypes.c_int, ctypes.c_int, _dp]),
     ("mpm_adjoint_backward", ctypes.c_int, [_hp, _dp, _dp, _dp]),
     ("mpm_adjoint_state", ctypes.c_int, [_hp, _dp, ctypes.c_uint]),
+    ("mpm_adjoint", ctypes.c_int, [_hp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp]),
     ("mpm_sort_permutation_noalloc", ctypes.c_int,
      [_pp, ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p, _up, ctypes.c_void_p]),
     ("mpm_testing_set_p2g_variant", ctypes.c_int, [_hp, ctypes.c_int]),

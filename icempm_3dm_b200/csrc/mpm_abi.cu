@@ -1372,3 +1372,11 @@ extern "C" int mpm_adjoint_state(mpm_handle* h, double* adj, unsigned pitch) {
     CK(h, cudaStreamSynchronize(h->stream));
     return MPM_OK;
 }
+
+extern "C" int mpm_adjoint(mpm_handle* h, int nsteps, int ckpt_every, const double* dL_dforce, double* dL_dcohesion,
+                           double* dL_dE) {
+    if (!h || !dL_dforce) return MPM_ERR_ARG;
+    const int r = mpm_adjoint_forward(h, nsteps, ckpt_every, nullptr);
+    if (r) return r;
+    return mpm_adjoint_backward(h, dL_dforce, dL_dcohesion, dL_dE);
+}

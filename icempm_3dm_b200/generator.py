@@ -103,6 +103,10 @@ class BlockConfig:
     ind_radius: float = 0.05
     pad: int = 3                              # wall pad nodes per side
     halo: int = 0                             # GridHaloSize (one partition)
+    grains: int = 0                           # spherical grains above a lattice block (0: plain block)
+    grain_frac: float = 0.0                   # share of the particles in the grains
+    grain_r: tuple = (0.02, 0.06)             # grain radius range (uniform)
+    block_frac_y: float = 0.4                 # lattice block height / domain height (grains cases)
 
 
 CONFIGS = {
@@ -112,6 +116,10 @@ CONFIGS = {
     "block8m": BlockConfig("block8m", 8_000_000, (4.0, 1.0, 1.0), 0.01, 2, 5e-6, 2000, 1.0,
                            cohesion_sigma_log=0.3),
     "calib500k": BlockConfig("calib500k", 500_000, (1.0, 0.5, 0.5), 0.01, 3, 1e-5, 200, 0.2),
+    # non-uniform density: 70 % in a lattice block filling the lower 40 % of a
+    # 6.0 x 1.5 x 1.5 m domain, 30 % in 20,000 grains above it
+    "grains30m": BlockConfig("grains30m", 30_000_000, (6.0, 1.5, 1.5), 0.008, 4, 2e-6, 5000, 2.0,
+                             cohesion_sigma_log=0.5, grains=20_000, grain_frac=0.3),
 }
 
 
@@ -157,6 +165,8 @@ def make_params(cfg, n=None):
 def make_block(cfg, n=None):
     """(prms, soa, cohesion): soa is a (28, n) float64 host SoA in the
     reference layout; cohesion is None for uniform cohesion."""
+    if cfg.grains > 0:
+        return make_grains_block(cfg, n)
     n = cfg.n if n is None else n
     dims = cfg.dims
     if n != cfg.n:   # a smaller copy of the same block keeps the spacing
@@ -200,6 +210,78 @@ def make_block(cfg, n=None):
     return p, soa, cohesion
 
 
+def make_grains_block(cfg, n=None):
+    """The non-uniform stress case: (1 - grain_frac) of the particles on a
+    jittered lattice filling the lower block_frac_y of the domain (placed as
+    make_block places a block), grain_frac of them in cfg.grains spheres with
+    radii uniform in cfg.grain_r whose centres are drawn uniformly (Poisson,
+    overlaps allowed) in the domain above the block; each sphere holds a share
+    of those particles proportional to its volume, spread uniformly inside it.
+    Every particle has the lattice's particle volume. A smaller n scales the
+    domain and the grain count with the particle count."""
+    n = cfg.n if n is None else n
+    if n != cfg.n:
+        scale = (n / cfg.n) ** (1.0 / 3.0)
+        cfg = dataclasses.replace(cfg, dims=tuple(d * scale for d in cfg.dims), n=n,
+                                  grains=max(1, int(round(cfg.grains * n / cfg.n))))
+    n_grain = int(round(n * cfg.grain_frac))
+    n_lat = n - n_grain
+    dom = np.asarray(cfg.dims, dtype=np.float64)
+    lat_dims = (dom[0], dom[1] * cfg.block_frac_y, dom[2])
+    p = make_params(cfg, n)
+    h = p.cellsize
+    lat = jittered_lattice(n_lat, lat_dims, cfg.seed)
+    box_x, box_z = p.GridXTotal * h, p.GridZ * h
+    x_off = (box_x - dom[0]) / 2
+    y_off = 2 * h
+    z_off = (box_z - dom[2]) / 2
+    lat[0] += x_off
+    lat[1] += y_off
+    lat[2] += z_off
+    # grains: radii, centres above the block, particle counts by volume
+    g = np.arange(cfg.grains, dtype=np.uint64)
+    r0, r1 = cfg.grain_r
+    rad = r0 + (r1 - r0) * uniform(cfg.seed, g, 21)
+    lat_top = y_off + lat_dims[1]
+    cx = x_off + rad + (dom[0] - 2 * rad) * uniform(cfg.seed, g, 22)
+    cy = lat_top + rad + (y_off + dom[1] - lat_top - 2 * rad) * uniform(cfg.seed, g, 23)
+    cz = z_off + rad + (dom[2] - 2 * rad) * uniform(cfg.seed, g, 24)
+    vol = rad ** 3
+    counts = np.floor(n_grain * vol / vol.sum()).astype(np.int64)
+    short = n_grain - int(counts.sum())
+    counts[np.argsort(-(n_grain * vol / vol.sum() - counts))[:short]] += 1
+    owner = np.repeat(np.arange(cfg.grains), counts)
+    pid = np.arange(n_grain, dtype=np.uint64) + np.uint64(n_lat)
+    d = np.stack([normal(cfg.seed, pid, 31 + k) for k in range(3)])
+    d /= np.maximum(np.linalg.norm(d, axis=0), 1e-300)
+    rr = rad[owner] * np.cbrt(uniform(cfg.seed, pid, 34))
+    gpos = np.stack([cx[owner], cy[owner], cz[owner]]) + d * rr
+    pos = np.concatenate([lat, gpos], axis=1)
+
+    mins, maxs = pos.min(axis=1), pos.max(axis=1)
+    p.xmin, p.ymin, p.zmin = mins
+    p.xmax, p.ymax, p.zmax = maxs
+    block_left = x_off
+    r = p.IndDiameter / 2
+    ht = r - p.IndDepth
+    p.indenter_x = math.floor((block_left - math.sqrt(r * r - ht * ht)) / h) * h
+    p.indenter_y = lat_top + ht
+    p.indenter_x_initial = p.indenter_x
+    p.indenter_y_initial = p.indenter_y
+    p.Volume = float(np.prod(lat_dims)) * n / n_lat
+    p.ParticleVolume = float(np.prod(lat_dims)) / n_lat
+    LIB.mpm_params_compute_helper_variables(p)
+
+    soa = np.zeros((N_PTS_ARRAYS, n), dtype=np.float64)
+    soa[POSX:POSX + 3] = pos
+    soa[IDX_JP_INV] = 1.0
+    for i in range(3):
+        soa[FE00 + 4 * i] = 1.0
+    z = normal(cfg.seed, np.arange(n, dtype=np.uint64), 11)
+    cohesion = cfg.cohesion_median * np.exp(cfg.cohesion_sigma_log * z)
+    return p, soa, cohesion
+
+
 def small_block(n=4000, seed=5, dims=(0.2, 0.1, 0.1), h=0.01, dt=1e-5, ind_velocity=0.2,
                 cohesion_sigma_log=0.0, youngs=5e8):
     """A small block for parity tests (seconds on the oracle)."""
@@ -222,5 +304,6 @@ def calibration_block(n=20_000, penetration_cells=3, ind_velocity=2.0, cohesion_
     return prms, soa, coh
 
 
-__all__ = ["BlockConfig", "CONFIGS", "make_block", "make_params", "small_block", "calibration_block",
+__all__ = ["BlockConfig", "CONFIGS", "make_block", "make_grains_block", "make_params", "small_block",
+           "calibration_block",
            "jittered_lattice", "splitmix64", "uniform", "normal", "BP00"]

@@ -190,6 +190,11 @@ int  mpm_adjoint_backward(mpm_handle* h, const double* dL_dforce, double* dL_dco
 /* Adjoints of the initial particle state after mpm_adjoint_backward: 25 rows
  * [x(3), v(3), C(9), F(9), Jp_inv] of row stride pitch >= n. */
 int  mpm_adjoint_state(mpm_handle* h, double* adj, unsigned pitch);
+/* Both sweeps in one call for a loss linear in the force history (dL_dforce
+ * known before the run): mpm_adjoint_forward(h, nsteps, ckpt_every, NULL)
+ * then mpm_adjoint_backward(h, dL_dforce, dL_dcohesion, dL_dE). */
+int  mpm_adjoint(mpm_handle* h, int nsteps, int ckpt_every, const double* dL_dforce, double* dL_dcohesion,
+                 double* dL_dE);
 
 /* No counterpart in the reference. The stable cell-key sort of mpm_sort
  * (same keys, same permutation) for callers that must not have the library

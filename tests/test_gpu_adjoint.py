@@ -152,3 +152,20 @@ def test_adjoint_matches_dual_number_forward_mode():
     for name, t, a in report:
         assert t != 0.0, name
         assert abs(t - a) <= 1e-6 * abs(t), (name, t, a)
+
+
+def test_single_call_adjoint_equals_forward_then_backward():
+    nsteps, every = 6, 2
+    prms, soa, coh = case()
+    n = soa.shape[1]
+    wgt = np.random.default_rng(5).standard_normal((nsteps, 3))
+    _, dc2, dE2, _ = adjoint(prms, soa, coh, wgt, nsteps, every)
+    with MPMHandle(prms, n, PRECISION_FP64_SVD64) as h:
+        h.upload(soa, cohesion=coh)
+        dc = np.zeros(n)
+        dE = ctypes.c_double(0)
+        w = np.ascontiguousarray(wgt)
+        check(LIB.mpm_adjoint(h._h, nsteps, every, dptr(w), dptr(dc), ctypes.byref(dE)), "mpm_adjoint")
+    # two GPU runs differ only by the summation order of FP64 atomics
+    assert np.allclose(dc, dc2, rtol=1e-8, atol=1e-8 * np.abs(dc2).max())
+    assert dE.value == pytest.approx(dE2, rel=1e-8)
