@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=45.0)
+    ap.add_argument("--adjoint", action="store_true",
+                    help="time the adjoint (forward with checkpoints + reverse sweep) on the calibration workload")
+    ap.add_argument("--ckpt-every", type=int, default=20)
     return ap.parse_args()
 
 
@@ -352,10 +355,60 @@ def run_ours(args):
     return 0
 
 
+def run_adjoint(args):
+    """One JSON line: the adjoint of the FP64 step (mpm_adjoint_forward with a
+    checkpoint every --ckpt-every substeps, then mpm_adjoint_backward) on the
+    calibration workload (default calib500k: 500,000 particles, 200 substeps),
+    as particle-steps/s of forward + reverse together, beside the plain FP64
+    step on the same block. CUDA events on the handle's stream."""
+    import torch
+    from icempm_3dm_b200 import MPMHandle, PRECISION_FP64_SVD64
+    from icempm_3dm_b200 import generator as gen
+    torch.cuda.set_device(0)
+    cfg = gen.CONFIGS[args.workload if args.workload != "block8m" else "calib500k"]
+    prms, soa, coh = gen.make_block(cfg)
+    if coh is None:
+        coh = cfg.cohesion_median * np.ones(soa.shape[1])
+    n = soa.shape[1]
+    steps = args.steps if args.steps != 1500 else cfg.steps
+    stream = torch.cuda.Stream()
+    h = MPMHandle(prms, n, PRECISION_FP64_SVD64)
+    h.set_stream(stream.cuda_stream)
+    rng = np.random.default_rng(0)
+    w = rng.standard_normal((steps, 3))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    h.upload(soa, cohesion=coh)
+    h.step(max(args.warmup, 3))
+    h.upload(soa, cohesion=coh)
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    h.step(steps)
+    ev[1].record(stream)
+    h.upload(soa, cohesion=coh)
+    torch.cuda.synchronize()
+    ev[2].record(stream)
+    h.adjoint_forward(steps, args.ckpt_every)
+    h.adjoint_backward(w)
+    ev[3].record(stream)
+    ev[3].synchronize()
+    t_fwd = ev[0].elapsed_time(ev[1])
+    t_adj = ev[2].elapsed_time(ev[3])
+    h.close()
+    out = {"metric": "adjoint particle-steps/s (forward with checkpoints + reverse)",
+           "value": n * steps / (t_adj * 1e-3), "unit": "particle-steps/s", "n_gpus": 1, "steps": steps,
+           "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": cfg.name, "particles": n, "ckpt_every": args.ckpt_every},
+           "ms_adjoint": t_adj, "ms_plain_fp64_forward": t_fwd, "adjoint_over_forward": t_adj / t_fwd}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.adjoint:
+        return run_adjoint(args)
     return run_ours(args)
 
 
