@@ -9,7 +9,7 @@
 //                  the identity, so that J - 1 and dev(F F^T) keep their
 //                  relative precision near the undeformed state)
 //   float   C[9]   APIC affine matrix ("Bp")
-//   float   Jp_inv
+//   float   Jp_inv - 1
 //   int32   status (low 32 bits of the reference's utility word)
 // optional float p0 (apex shift from cohesion), and float P, Q rows written
 // on record steps.
@@ -35,7 +35,7 @@ struct MixedState {
     float* v;        // 3 rows
     float* E;        // 9 rows
     float* C;        // 9 rows
-    float* Jp;       // 1 row
+    float* Jpm1;     // Jp_inv - 1 (1 row): keeps the precision of Jp_inv near 1
     int* status;     // 1 row
     float* p0;       // 1 row or null
     float* PQ;       // 2 rows (P, Q)
@@ -520,7 +520,7 @@ __device__ __forceinline__ void g2p_gather_tma(const DevParams& P, const WarpBox
 // value so that nothing of the caller is forced into local memory.
 struct ElasticState {
     float e[9];   // F - I, row-major
-    float jp;     // Jp_inv
+    float jp;     // Jp_inv - 1
 };
 
 __device__ __noinline__ ElasticState return_map_f64(const DPParams P, const ElasticState in, const double p0) {
@@ -531,10 +531,10 @@ __device__ __noinline__ ElasticState return_map_f64(const DPParams P, const Elas
         for (int j = 0; j < 3; j++) F[i][j] = (i == j ? 1.0 : 0.0) + (double)in.e[3 * i + j];
     double Je, p_tr, q_tr;
     trial_pq(P, F, Je, p_tr, q_tr);
-    double jp = in.jp;
+    double jp = 1.0 + (double)in.jp;
     drucker_prager_return<SvdF64>(P, F, jp, Je, p_tr, q_tr, p0);
     ElasticState out;
-    out.jp = (float)jp;
+    out.jp = (float)(jp - 1.0);
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -874,12 +874,14 @@ __device__ __forceinline__ bool p2g_scatter_tile_fx(const DevParams& P, float4* 
 
 // P2G payload of a particle: S = m C - dt V Dp^-1 tau (mpm_kernels.cuh:63)
 __device__ __forceinline__ void p2g_payload_mixed(const DevParams& P, const float E[3][3], const float C[3][3],
-                                                  const float v[3], bool liquid, float Jp, float& mass, float mv[3],
+                                                  const float v[3], bool liquid, float Jpm1, float& mass, float mv[3],
                                                   float S[3][3]) {
     mass = (float)(liquid ? P.liquid_mass : P.particle_mass);
     float tau[3][3];
     if (liquid) {
-        const float pw = (float)P.kappa * (1.0f - 1.0f / (Jp * Jp * Jp));
+        // kappa (1 - J^-3) with J = 1 + d: (J^3 - 1) / J^3 = d (3 + 3d + d^2) / J^3, free of cancellation
+        const float J = 1.0f + Jpm1;
+        const float pw = (float)P.kappa * (Jpm1 * (3.0f + Jpm1 * (3.0f + Jpm1)) / (J * J * J));
 #pragma unroll
         for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -896,14 +898,14 @@ __device__ __forceinline__ void p2g_payload_mixed(const DevParams& P, const floa
     }
 }
 
-__device__ __forceinline__ void load_mixed(const MixedState& s, int i, int X[3], float E[3][3], float& Jp, int& st) {
+__device__ __forceinline__ void load_mixed(const MixedState& s, int i, int X[3], float E[3][3], float& Jpm1, int& st) {
 #pragma unroll
     for (int d = 0; d < 3; d++) X[d] = s.X[d * s.pitch + i];
 #pragma unroll
     for (int r = 0; r < 3; r++)
 #pragma unroll
         for (int c = 0; c < 3; c++) E[r][c] = s.E[(3 * r + c) * s.pitch + i];
-    Jp = s.Jp[i];
+    Jpm1 = s.Jpm1[i];
     st = s.status[i];
 }
 
@@ -914,8 +916,8 @@ __global__ void __launch_bounds__(256) k_p2g_mixed(DevParams P, MixedState s, in
     const int lane = threadIdx.x & 31;
     bool active = i < n;
     int X[3] = {0, 0, 0}, st = (int)kDisabled;
-    float E[3][3], Jp = 1.f;
-    if (active) load_mixed(s, i, X, E, Jp, st);
+    float E[3][3], Jpm1 = 0.f;
+    if (active) load_mixed(s, i, X, E, Jpm1, st);
     active = active && !(st & (int)kDisabled);
     int base[3];
     float fx[3], mass = 0.f, mv[3] = {0, 0, 0}, S[3][3];
@@ -930,7 +932,7 @@ __global__ void __launch_bounds__(256) k_p2g_mixed(DevParams P, MixedState s, in
         for (int r = 0; r < 3; r++)
 #pragma unroll
             for (int c = 0; c < 3; c++) C[r][c] = s.C[(3 * r + c) * s.pitch + i];
-        p2g_payload_mixed(P, E, C, v, (st & (int)kLiquid) != 0, Jp, mass, mv, S);
+        p2g_payload_mixed(P, E, C, v, (st & (int)kLiquid) != 0, Jpm1, mass, mv, S);
         const int e = stencil_error(P, base[0], base[1], base[2]);
         if (e) raise_error(err, e);
         inside = e == 0;
@@ -950,8 +952,8 @@ __global__ void __launch_bounds__(256) k_p2g_mixed(DevParams P, MixedState s, in
 // only when store_vc or crushed (the next G2P recomputes them from the grid);
 // Jp_inv and status only when they changed.
 __device__ __forceinline__ bool fused_update_state(const DevParams& P, const MixedState& s, int i, bool active,
-                                                   int X[3], int& st, int st_in, float jp_in, float E[3][3],
-                                                   float& Jp, const float v[3], const float C[3][3],
+                                                   int X[3], int& st, int st_in, float jpm1_in, float E[3][3],
+                                                   float& Jpm1, const float v[3], const float C[3][3],
                                                    ElasticInv& inv, int record_pq, int store_vc,
                                                    int* __restrict__ rm_list, int* __restrict__ rm_count, int lane) {
     bool need_rm = false;
@@ -973,7 +975,8 @@ __device__ __forceinline__ bool fused_update_state(const DevParams& P, const Mix
             for (int r = 0; r < 3; r++)
 #pragma unroll
                 for (int c = 0; c < 3; c++) A[r][c] = dt * C[r][c];
-            Jp *= 1.0f + detm1(A);
+            const float dA = detm1(A);   // det(I + dt C) - 1
+            Jpm1 = Jpm1 + dA + Jpm1 * dA;     // Jp_inv <- Jp_inv det(I + dt C), as Jp_inv - 1
 #pragma unroll
             for (int r = 0; r < 3; r++)
 #pragma unroll
@@ -1016,7 +1019,7 @@ __device__ __forceinline__ bool fused_update_state(const DevParams& P, const Mix
 #pragma unroll
                 for (int c = 0; c < 3; c++) s.C[(3 * r + c) * s.pitch + i] = C[r][c];
         }
-        if (__float_as_int(Jp) != __float_as_int(jp_in)) s.Jp[i] = Jp;
+        if (__float_as_int(Jpm1) != __float_as_int(jpm1_in)) s.Jpm1[i] = Jpm1;
         if (st != st_in) s.status[i] = st;
     }
     return need_rm;
@@ -1025,7 +1028,7 @@ __device__ __forceinline__ bool fused_update_state(const DevParams& P, const Mix
 // P2G payload of the fused kernels (S = m C - dt V Dp^-1 tau, mpm_kernels.cuh:63)
 // at the advected position; inactive lanes get a zero payload.
 __device__ __forceinline__ void fused_payload(const DevParams& P, bool active, const int X[3], int st,
-                                              const float E[3][3], const float C[3][3], const float v[3], float Jp,
+                                              const float E[3][3], const float C[3][3], const float v[3], float Jpm1,
                                               const ElasticInv& inv, int base[3], float fx[3], float& mass,
                                               float mv[3], float S[3][3], bool& inside, int* err) {
     mass = 0.f;
@@ -1034,7 +1037,7 @@ __device__ __forceinline__ void fused_payload(const DevParams& P, bool active, c
 #pragma unroll
         for (int d = 0; d < 3; d++) fix_base(X[d], base[d], fx[d]);
         if (st & (int)kLiquid) {
-            p2g_payload_mixed(P, E, C, v, true, Jp, mass, mv, S);
+            p2g_payload_mixed(P, E, C, v, true, Jpm1, mass, mv, S);
         } else {
             mass = (float)P.particle_mass;
             float tau[3][3];
@@ -1084,7 +1087,7 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     const int lane = threadIdx.x & 31;
     bool active = i < n;
     int X[3] = {0, 0, 0}, st = (int)kDisabled;
-    float E[3][3], Jp = 1.f;
+    float E[3][3], Jpm1 = 0.f;
     // positions and status first: the gather box (and its copy) depends on them
     if (active) {
         st = s.status[i];
@@ -1113,10 +1116,10 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
         for (int r = 0; r < 3; r++)
 #pragma unroll
             for (int c = 0; c < 3; c++) E[r][c] = s.E[(3 * r + c) * s.pitch + i];
-        Jp = s.Jp[i];
+        Jpm1 = s.Jpm1[i];
     }
     const int st_in = st;
-    const float jp_in = Jp;
+    const float jpm1_in = Jpm1;
     if (GATHER == 2) {
         g2p_gather_tma<kTmaSliceNodes>(P, wbox, vel, vbox_tma, &vbox_bar[threadIdx.x >> 5], active && e0 == 0,
                                        active, base, fx, v, C, lane, wx, err);
@@ -1126,12 +1129,12 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     } else if (active) {
         g2p_gather_mixed(P, vel, base, fx, v, C, e0 != 0, wx);
     }
-    const bool need_rm = fused_update_state(P, s, i, active, X, st, st_in, jp_in, E, Jp, v, C, inv, record_pq,
+    const bool need_rm = fused_update_state(P, s, i, active, X, st, st_in, jpm1_in, E, Jpm1, v, C, inv, record_pq,
                                             store_vc, rm_list, rm_count, lane);
     active = active && !need_rm;   // crushed points scatter in k_return_map_mixed
     if (!do_p2g) return;   // uniform across the launch
     float mass, mv[3], S[3][3];
-    fused_payload(P, active, X, st, E, C, v, Jp, inv, base, fx, mass, mv, S, inside, err);
+    fused_payload(P, active, X, st, E, C, v, Jpm1, inv, base, fx, mass, mv, S, inside, err);
     if (SCATTER == 2 && p2g_scatter_tile<128>(P, acc, mixed_tile, tile_cap, active, inside, base, fx, mass, mv, S, lane))
         return;
     if (SCATTER == 3 && p2g_scatter_tile_fx<128>(P, acc, reinterpret_cast<int*>(mixed_tile), tile_cap, active, inside,
@@ -1155,20 +1158,20 @@ __global__ void __launch_bounds__(128) k_return_map_mixed(DevParams P, MixedStat
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
         const int i = rm_list[k];
         int X[3], st;
-        float E[3][3], Jp;
-        load_mixed(s, i, X, E, Jp, st);
+        float E[3][3], Jpm1;
+        load_mixed(s, i, X, E, Jpm1, st);
         const double p0 = s.p0 ? (double)s.p0[i] : P.p0;
         ElasticState es;
 #pragma unroll
         for (int q = 0; q < 9; q++) es.e[q] = E[q / 3][q % 3];
-        es.jp = Jp;
+        es.jp = Jpm1;
         es = return_map_f64(dp_params(P), es, p0);
 #pragma unroll
         for (int q = 0; q < 9; q++) {
             E[q / 3][q % 3] = es.e[q];
             s.E[q * s.pitch + i] = es.e[q];
         }
-        if (__float_as_int(es.jp) != __float_as_int(Jp)) s.Jp[i] = es.jp;
+        if (__float_as_int(es.jp) != __float_as_int(Jpm1)) s.Jpm1[i] = es.jp;
         if (!do_p2g) continue;
         float v[3], C[3][3], mass, mv[3], S[3][3], fx[3];
         int base[3];
@@ -1293,7 +1296,7 @@ __global__ void k_mixed_from_f64(const double* __restrict__ src, size_t spitch, 
             s.E[(3 * r + c) * s.pitch + i] = (float)(src[(MPM_FE00 + 3 * r + c) * spitch + i] - (r == c ? 1.0 : 0.0));
             s.C[(3 * r + c) * s.pitch + i] = (float)src[(MPM_BP00 + 3 * r + c) * spitch + i];
         }
-    s.Jp[i] = (float)src[MPM_IDX_JP_INV * spitch + i];
+    s.Jpm1[i] = (float)(src[MPM_IDX_JP_INV * spitch + i] - 1.0);
     s.status[i] = (int)__double_as_longlong(src[i]);
     s.PQ[i] = (float)src[MPM_IDX_P * spitch + i];
     s.PQ[s.pitch + i] = (float)src[MPM_IDX_Q * spitch + i];
@@ -1316,7 +1319,7 @@ __global__ void k_mixed_to_f64(MixedState s, int n, double* __restrict__ dst, si
             dst[(MPM_FE00 + 3 * r + c) * dpitch + i] = (double)s.E[(3 * r + c) * s.pitch + i] + (r == c ? 1.0 : 0.0);
             dst[(MPM_BP00 + 3 * r + c) * dpitch + i] = (double)s.C[(3 * r + c) * s.pitch + i];
         }
-    dst[MPM_IDX_JP_INV * dpitch + i] = (double)s.Jp[i];
+    dst[MPM_IDX_JP_INV * dpitch + i] = 1.0 + (double)s.Jpm1[i];
     const long long hi = __double_as_longlong(dst[i]) & (long long)0xffffffff00000000LL;
     dst[i] = __longlong_as_double(hi | (long long)(unsigned)s.status[i]);
     dst[MPM_IDX_P * dpitch + i] = (double)s.PQ[i];

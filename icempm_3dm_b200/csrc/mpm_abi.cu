@@ -236,7 +236,7 @@ MixedState mixed_state(mpm_handle* h) {
     m.v = wf + 3 * p;
     m.E = wf + 6 * p;
     m.C = wf + 15 * p;
-    m.Jp = wf + 24 * p;
+    m.Jpm1 = wf + 24 * p;
     m.status = wi + 25 * p;
     m.PQ = wf + 26 * p;
     m.p0 = h->p0f;

@@ -142,3 +142,52 @@ def test_split_calls_and_periodic_sort_keep_state():
         assert rel_dev(full[BP00:BP00 + 9], sim.soa[BP00:BP00 + 9]) < 1e-3
     (h1, f1), (h2, f2) = outs
     assert np.abs(f1[VELX:VELX + 3] - f2[VELX:VELX + 3]).max() < 1e-4 * np.abs(f1[VELX:VELX + 3]).max()
+
+
+@pytest.mark.parametrize("scatter,gather", [(9, 5), (6, 2)])
+def test_liquid_and_disabled_particles_in_the_fused_path(scatter, gather):
+    """Water points (status 0x40000: Kirchhoff stress replaced by the water
+    pressure, Jp_inv advected by det(I + dt C)) and disabled points (skipped)
+    through the mixed fused kernel, against the FP64-SVD oracle."""
+    from icempm_3dm_b200._lib import STATUS_DISABLED
+    from tests.helpers import util_as_double
+    prms, soa = perturbed_block(n=4000, seed=91, liquid_frac=0.15, crushed_frac=0.05, strong_frac=0.0,
+                                ind_velocity=0.5)
+    n = soa.shape[1]
+    bits = util_bits(soa).copy()
+    # water starts unstrained (Jp_inv = 1): a block's "tension" points made
+    # liquid would start as water under -6 MPa, a state whose dynamics amplify
+    # any rounding difference (mixed and FP64 then part within 20 substeps)
+    # and without the block's random affine field (std 5 1/s), which compresses the
+    # water by tens of per cent within 30 substeps
+    soa[IDX_JP_INV, (bits & (1 << 18)) != 0] = 1.0
+    soa[BP00:BP00 + 9, (bits & (1 << 18)) != 0] = 0.0
+    dis = np.random.default_rng(3).random(n) < 0.05
+    bits[dis] |= STATUS_DISABLED
+    soa[IDX_UTILITY] = util_as_double(bits)
+    steps = 30
+    with MPMHandle(prms, n, PRECISION_MIXED) as h:
+        h.set_p2g_variant(scatter)
+        h.set_g2p_variant(gather)
+        h.upload(soa)
+        held = h.download()         # the state as the mixed handle holds it (FP32 rounding)
+        hist = h.step(steps)
+        out = h.download()
+    sim = po.OracleSim(prms, soa, n, svd_mode=1)
+    ref_hist, err = sim.step(steps)
+    assert err == 0
+    assert np.linalg.norm(hist - ref_hist) / np.linalg.norm(ref_hist) < 1e-3
+    live = ~dis
+    assert np.array_equal(out[:, dis], held[:, dis])              # disabled points untouched
+    # positions: FP32 state in a block with holes and a random affine field
+    # (std 5 1/s) on its solid points; 1.2e-6 m measured after 30 substeps
+    xdev = np.abs(out[POSX:POSX + 3, live] - sim.soa[POSX:POSX + 3, live]).max()
+    assert xdev < 5e-6, xdev
+    liquid = (bits & (1 << 18)) != 0
+    # water Jp_inv: compared where no return map can touch it (not crushed)
+    crushed_any = ((util_bits(out) | util_bits(sim.soa)) & STATUS_CRUSHED) != 0
+    wl = live & liquid & ~crushed_any
+    assert wl.sum() > 100
+    # the reference's water uses the ice bulk modulus (kappa ~ 4e8 Pa): its points
+    # reach J = 0.87..1.45 here, and Jp_inv follows the oracle to 2e-3 of that
+    assert rel_dev(out[IDX_JP_INV, wl], sim.soa[IDX_JP_INV, wl]) < 2e-3
