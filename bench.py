@@ -273,7 +273,7 @@ def run_ours(args):
             active * B_NODE["mixed"]
         launches_per_step = 3
     else:
-        names = ["grid clear", "k_p2g_warpagg_f64", "k_update_f64", "k_g2p_f64"]
+        names = ["grid clear", "k_p2g_pairs_f64", "k_update_f64", "k_g2p_f64"]
         k = int(np.argmax(kms[1:])) + 1
         dom_name, dom_ms = names[k], kms[k] / args.steps
         # FP64 form: P2G reads 200 B (x, v, F, C), G2P reads 112 B and writes 208 B

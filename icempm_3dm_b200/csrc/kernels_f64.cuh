@@ -197,6 +197,50 @@ __global__ void k_p2g_warpagg_f64(DevParams P, const double* __restrict__ pts, s
     });
 }
 
+// Variant 5: lanes that share a base cell merged in pairs by one shuffle
+// round per node (cell-sorted order puts them in neighbouring lanes; the
+// odd-ranked partner's four sums go to the even-ranked lane, which issues the
+// FP64 atomics for both), 128-thread blocks at MINB blocks per SM.
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_p2g_pairs_f64(DevParams P, const double* __restrict__ pts, size_t pitch,
+                                                             int n, double* __restrict__ grid, int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    P2GPoint q;
+    bool active = (i < n) && p2g_prepare(P, pts, pitch, i, q, err);
+    const bool inside = active && !stencil_error(P, q.base[0], q.base[1], q.base[2]);
+    if (!inside) {
+        q.mass = 0;
+        if (!active) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) { q.base[d] = 0; q.fx[d] = 1.0; q.mv[d] = 0; }
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) q.S[r][c] = 0;
+        }
+    }
+    const long long key = base_key(P, q, inside, lane);
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    const long long next_key = __shfl_down_sync(0xffffffffu, key, 1);
+    const bool absorb = lane < 31 && next_key == key && (rank & 1) == 0;
+    const bool absorbed = __shfl_up_sync(0xffffffffu, (int)absorb, 1) != 0 && lane > 0;
+    p2g_scatter(P, q, [&](int a, int b, int c, double incM, const double incV[3]) {
+        double v[4] = {incM, incV[0], incV[1], incV[2]};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const double o = __shfl_down_sync(0xffffffffu, v[k], 1);
+            if (absorb) v[k] += o;
+        }
+        if (!active || absorbed) return;
+        const int x = q.base[0] + a, y = q.base[1] + b, z = q.base[2] + c;
+        if (!inside && !node_inside(P, x, y, z)) return;
+        const double vv[3] = {v[1], v[2], v[3]};
+        grid_atomic_add(grid, P.gstride, node_index(P, x, y, z), v[0], vv);
+    });
+}
+
 // Shared-memory tile P2G (variants 0 and 3): the block's particles (a
 // contiguous range of the cell-sorted order) span a small box of nodes. The
 // block accumulates its box in shared memory (SoA, tile_cap nodes per

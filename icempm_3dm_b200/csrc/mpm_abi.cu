@@ -117,7 +117,7 @@ struct mpm_handle {
     int adj_steps = 0, adj_every = 0;
     bool adj_ready = false;
 
-    int p2g_variant = 2;              // see mpm_testing_set_p2g_variant
+    int p2g_variant = 5;              // see mpm_testing_set_p2g_variant (5: pair-merged, 6 per SM)
     int g2p_variant = 2;              // see mpm_testing_set_g2p_variant
     int tile_cap = 2048;              // P2G tile nodes (x 32 B of shared memory)
     int fx_tile_cap = 3072;           // nodes of the fixed-point tile (x 32 B)
@@ -283,6 +283,12 @@ int launch_p2g(mpm_handle* h) {
             break;
         case 2:
             k_p2g_warpagg_f64<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, h->err);
+            break;
+        case 5:
+            k_p2g_pairs_f64<6><<<blocks_for(n, 128), 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, h->err);
+            break;
+        case 6:
+            k_p2g_pairs_f64<4><<<blocks_for(n, 128), 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, h->err);
             break;
         case 3:
             k_p2g_tile_f64<256, true><<<blocks_for(n, 256), 256, smem, h->stream>>>(h->dp, h->pts, h->pitch, n,
@@ -1101,10 +1107,12 @@ int mpm_testing_download_grid(mpm_handle* h, double* out, int which) {
 
 int mpm_testing_set_p2g_variant(mpm_handle* h, int variant) {
     if (!h || variant < 0 || variant > 9) return MPM_ERR_ARG;
-    if (variant >= 5) {
+    if (is_mixed(h)) {
+        if (variant < 5) return MPM_ERR_ARG;
         h->mixed_scatter = variant - 5;
         return MPM_OK;
     }
+    if (variant > 6) return MPM_ERR_ARG;
     h->p2g_variant = variant;
     return MPM_OK;
 }
@@ -1338,7 +1346,7 @@ extern "C" int mpm_adjoint_backward(mpm_handle* h, const double* dL_dforce, doub
             const double* Sn1 = h->seg[s - s0 + 1];
             const double ix = sp[s - s0].indenter_x, iy = sp[s - s0].indenter_y;
             CK(h, cudaMemsetAsync(h->adj_g7, 0, sizeof(double) * 4 * gs, h->stream));
-            k_p2g_warpagg_f64<<<blocks_for(n, 256), 256, 0, h->stream>>>(dp, Sn, h->pitch, n, h->adj_g7, h->err);
+            k_p2g_pairs_f64<6><<<blocks_for(n, 128), 128, 0, h->stream>>>(dp, Sn, h->pitch, n, h->adj_g7, h->err);
             k_adj_update_record<256><<<blocks_for(dp.nodes, 256), 256, 0, h->stream>>>(dp, h->adj_g7, ix, iy);
             CK(h, cudaMemsetAsync(h->adj_gb7, 0, sizeof(double) * 7 * gs, h->stream));
             k_adj_g2p_rev<128><<<blocks_for(n, 128), 128, 0, h->stream>>>(dp, q, Sn, Sn1, h->pitch, n, h->adj_g7, h->p0,

@@ -16,8 +16,10 @@ extern "C" {
  * with one flush per tile node, 1 = one thread per particle with 27x4
  * global atomics, 2 = as 1 with a warp reduction over particles sharing a
  * base cell, 3 = as 0 with that warp reduction, 4 = shared-memory tile in
- * 64-bit block fixed point over 1024-particle chunks. In the mixed mode,
- * 5..8 select the fused kernel's scatter: 5 = warp-reduced float4 atomics,
+ * 64-bit block fixed point over 1024-particle chunks, 5 (default) and 6 =
+ * as 1 with same-cell particle pairs merged by one shuffle round
+ * (128-thread blocks, 6 and 4 per SM). In the mixed mode (where 0..4 give MPM_ERR_ARG) 5..9
+ * select the fused kernel's scatter: 5 = warp-reduced float4 atomics,
  * 6 = float4 atomics per particle, 7 = FP32 shared-memory tile,
  * 8 = int32 block fixed-point shared-memory tile, 9 = float4 atomics with
  * same-cell particle pairs merged in registers (default). */

@@ -105,7 +105,7 @@ def one_phase_step(prms, soa, record=True, p0=None, precision=PRECISION_FP64, va
     return g_p2g, g_upd, out, sensor
 
 
-@pytest.mark.parametrize("variant,g2p_variant", [(0, 0), (1, 1), (2, 2), (3, 0)])
+@pytest.mark.parametrize("variant,g2p_variant", [(0, 0), (1, 1), (2, 2), (3, 0), (5, 2), (6, 2)])
 def test_single_step_phases_match_oracle(variant, g2p_variant):
     prms, soa = perturbed_block(n=4000, seed=31)
     n = soa.shape[1]
