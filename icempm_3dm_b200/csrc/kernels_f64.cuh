@@ -577,39 +577,58 @@ __device__ __forceinline__ void g2p_gather(const DevParams& P, const double* __r
     if (e) raise_error(err, e);
     double ww[3][3];
     quad_weights<double>(fx, ww);
+    // v = sum w v_i and the first moments M_k = sum w v_i o_k over the node
+    // offsets o = (a, b, c); C = 4/h sum w v_i (o - f) = 4/h (M - f v)
+    double Mx[3], My[3], Mz[3];
 #pragma unroll
-    for (int d = 0; d < 3; d++) {
-        vel[d] = 0;
-#pragma unroll
-        for (int k = 0; k < 3; k++) C[d][k] = 0;
-    }
-    const double s4 = 4. * P.h_inv;
+    for (int d = 0; d < 3; d++) { vel[d] = 0; Mx[d] = 0; My[d] = 0; Mz[d] = 0; }
     const long long i0 = node_index(P, base[0], base[1], base[2]);
     const double* gx = grid + P.gstride;
     const double* gy = grid + 2 * P.gstride;
     const double* gz = grid + 3 * P.gstride;
 #pragma unroll 1
-    for (int a = 0; a < 3; a++)
+    for (int a = 0; a < 3; a++) {
+        const double wa = a == 0 ? ww[0][0] : (a == 1 ? ww[1][0] : ww[2][0]);
+        double ra[3] = {0, 0, 0};
 #pragma unroll
         for (int b = 0; b < 3; b++) {
             const long long ib = i0 + a * P.slab + b * P.Gz;
+            const double wab = wa * ww[b][1];
+            double rb[3] = {0, 0, 0};
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const int x = base[0] + a, y = base[1] + b, z = base[2] + c;
                 if (e && !node_inside(P, x, y, z)) continue;
                 const long long ni = ib + c;
-                const double w = ww[a][0] * ww[b][1] * ww[c][2];
-                const double nv[3] = {__ldg(gx + ni), __ldg(gy + ni), __ldg(gz + ni)};
-                const double dp[3] = {a - fx[0], b - fx[1], c - fx[2]};
-                const double sw = s4 * w;
+                const double w = wab * ww[c][2];
+                const double wn[3] = {w * __ldg(gx + ni), w * __ldg(gy + ni), w * __ldg(gz + ni)};
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
-                    vel[r] += w * nv[r];
-#pragma unroll
-                    for (int k = 0; k < 3; k++) C[r][k] += sw * (nv[r] * dp[k]);
+                    rb[r] += wn[r];
+                    if (c == 1) Mz[r] += wn[r];
+                    if (c == 2) Mz[r] += 2.0 * wn[r];
                 }
             }
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                ra[r] += rb[r];
+                if (b == 1) My[r] += rb[r];
+                if (b == 2) My[r] += 2.0 * rb[r];
+            }
         }
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            vel[r] += ra[r];
+            Mx[r] += (double)a * ra[r];
+        }
+    }
+    const double s4 = 4. * P.h_inv;
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        C[r][0] = s4 * (Mx[r] - fx[0] * vel[r]);
+        C[r][1] = s4 * (My[r] - fx[1] * vel[r]);
+        C[r][2] = s4 * (Mz[r] - fx[2] * vel[r]);
+    }
 }
 
 // The particle update after the gather (mpm_kernels.cuh:307-327).

@@ -118,7 +118,7 @@ struct mpm_handle {
     bool adj_ready = false;
 
     int p2g_variant = 5;              // see mpm_testing_set_p2g_variant (5: pair-merged, 6 per SM)
-    int g2p_variant = 2;              // see mpm_testing_set_g2p_variant
+    int g2p_variant = 0;              // see mpm_testing_set_g2p_variant (0: 4 blocks of 128 per SM)
     int tile_cap = 2048;              // P2G tile nodes (x 32 B of shared memory)
     int fx_tile_cap = 3072;           // nodes of the fixed-point tile (x 32 B)
     float* chunk_bound = nullptr;     // per-chunk |contribution| bound of the fixed-point P2G

@@ -26,7 +26,7 @@ extern "C" {
 int mpm_testing_set_p2g_variant(mpm_handle* h, int variant);
 
 /* G2P kernel occupancy target (FP64 modes): 0 = 4 blocks of 128 threads per
- * SM, 1 = 3 blocks, 2 = 6 blocks (default; fewer registers per thread). In
+ * SM (default), 1 = 3 blocks, 2 = 6 blocks (fewer registers per thread). In
  * the mixed mode the fused kernel's target: 0 = 4, 1 = 5, 2 = 6 blocks;
  * 3 = 6, 4 = 5 and 5 = 8 blocks (default) with each warp's velocity box
  * staged in shared memory for the gather by the warp's loads, 6 = 8 blocks
