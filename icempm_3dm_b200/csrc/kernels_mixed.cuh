@@ -1,5 +1,5 @@
-// Mixed-precision step: FP32 particle state and transfers, FP64 where the
-// north-star requires it (3x3 SVD and return map of crushed particles,
+// Mixed-precision step: FP32 particle state and transfers, FP64 where
+// precision needs it (3x3 SVD and return map of crushed particles, the
 // indenter force reduction).
 //
 // Particle state (SoA, 26 words = 104 B per particle):
@@ -15,10 +15,12 @@
 // on record steps.
 //
 // Grid: acc = float4 {m, m vx, m vy, m vz} per node, accumulated with
-// warp-aggregated vector atomics; vel = float4 {vx, vy, vz, 0} per node,
-// written by the node update (which also clears acc for the next P2G).
-// One step is two kernels: node update, then the fused G2P->P2G kernel
-// (G2P of this step and P2G of the next read each particle once).
+// float4 vector atomics (same-cell particle pairs merged in registers first);
+// vel = float4 {vx, vy, vz, 0} per node, written by the node update (which
+// also clears acc for the next P2G).
+// One step is three kernels: node update, the fused G2P->P2G kernel (G2P of
+// this step and P2G of the next read each particle once), and the FP64
+// return map of the points that crushed (k_return_map_mixed, over a list).
 #pragma once
 
 #include "device_common.cuh"

@@ -1122,7 +1122,7 @@ int mpm_testing_set_p2g_variant(mpm_handle* h, int variant) {
 // ------------------------------------------- sort without device allocation
 //
 // Some callers cannot let a library allocate device memory: applications that
-// own and budget every byte of the GPU themselves (their own pool, a fixed
+// own and plan every byte of the GPU themselves (their own pool, a fixed
 // footprint planned at start-up), and loops that cannot afford the latency
 // and implicit device-wide synchronisation of a cudaMalloc in the middle of a
 // run. mpm_sort_permutation_noalloc serves them: the caller passes its own
