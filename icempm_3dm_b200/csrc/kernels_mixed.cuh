@@ -682,6 +682,133 @@ __device__ __forceinline__ void p2g_scatter_pairs(const DevParams& P, float4* __
     }
 }
 
+// One particle's stencil as a lane of the split scatter walks it: loop node
+// (a, b, c) is stencil node (a, b, c), or (2-a, 2-b, 2-c) when flipped. The
+// flip permutes the per-dimension weights already computed for the particle
+// (w_{2-k}(f) = w_k(2-f) for the quadratic B-spline), so each node gets the
+// same weight numbers as in the unsplit loop. The affine part is walked
+// incrementally: u = m v + S (x_node - x_p) at loop node (0,0,0), and each
+// loop step in a, b, c adds sh = +-h S[:,d] (minus when flipped).
+struct SplitStream {
+    float m, u[3], s0h[3], s1h[3], s2h[3], wa[2], wb[3], wc[3];
+};
+
+__device__ __forceinline__ void split_stream(const DevParams& P, SplitStream& H, float m, const float mv[3],
+                                             const float S[3][3], const float fx[3], bool flip) {
+    float ww[3][3];
+    quad_weights<float>(fx, ww);
+    const float h = (float)P.h;
+    const float sg = flip ? -h : h;
+    const float k0 = flip ? 2.0f : 0.0f;
+    H.m = m;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        H.wb[k] = flip ? ww[2 - k][1] : ww[k][1];
+        H.wc[k] = flip ? ww[2 - k][2] : ww[k][2];
+        if (k < 2) H.wa[k] = flip ? ww[2 - k][0] : ww[k][0];
+    }
+    const float d0 = (k0 - fx[0]) * h, d1 = (k0 - fx[1]) * h, d2 = (k0 - fx[2]) * h;
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        H.u[r] = mv[r] + S[r][0] * d0 + S[r][1] * d1 + S[r][2] * d2;
+        H.s0h[r] = S[r][0] * sg;
+        H.s1h[r] = S[r][1] * sg;
+        H.s2h[r] = S[r][2] * sg;
+    }
+}
+
+// Split scatter (SCATTER 5). Pairs as in p2g_scatter_pairs (two adjacent
+// lanes with the same base cell), but instead of shuffling 4 values per node
+// the pair exchanges its payloads once and each lane adds BOTH particles'
+// contributions over half of the 27 nodes: the first lane nodes 0..13 in
+// (a, b, c) order, the second the mirror images of its loop nodes 0..12,
+// i.e. nodes 26..14. A lone particle walks both halves itself, as two
+// streams: nodes 0..13, then the mirrored 26..14. Each lane runs 14 loop
+// nodes with two contributions each (27 of the 28 slots used) and one float4
+// atomic per node (pairs) or two (lone particles). Warps with a stencil
+// outside the grid take the checked loop of p2g_scatter_pairs.
+__device__ __forceinline__ void p2g_scatter_split(const DevParams& P, float4* __restrict__ acc, bool active,
+                                                  bool inside, const int base[3], const float fx[3], float mass,
+                                                  const float mv[3], const float S[3][3], int lane, WxSlot wx) {
+    if (!__all_sync(0xffffffffu, inside || !active)) {
+        p2g_scatter_pairs(P, acc, active, inside, base, fx, mass, mv, S, lane, wx);
+        return;
+    }
+    const int i0 = ((base[0] + P.halo) * P.Gy + base[1]) * P.Gz + base[2];
+    const int key = active ? i0 : -1 - lane;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    const int next_key = __shfl_down_sync(0xffffffffu, key, 1);
+    const bool first = lane < 31 && next_key == key && (rank & 1) == 0;
+    const bool second = __shfl_up_sync(0xffffffffu, (int)first, 1) != 0 && lane > 0;
+    const bool merged = first || second;
+    const int partner = first ? lane + 1 : (second ? lane - 1 : lane);
+    // the partner's payload (a lone lane reads its own)
+    float pm = __shfl_sync(0xffffffffu, mass, partner), pmv[3], pS[3][3], pfx[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        pmv[r] = __shfl_sync(0xffffffffu, mv[r], partner);
+        pfx[r] = __shfl_sync(0xffffffffu, fx[r], partner);
+#pragma unroll
+        for (int c = 0; c < 3; c++) pS[r][c] = __shfl_sync(0xffffffffu, S[r][c], partner);
+    }
+    // stream A: own particle, flipped on the second lane of a pair; stream B:
+    // the partner's particle on a pair's lanes (same flip), the own particle
+    // flipped on a lone lane (same base cell in every case)
+    SplitStream A, B;
+    split_stream(P, A, mass, mv, S, fx, second);
+    split_stream(P, B, pm, pmv, pS, pfx, !first);
+    const int slab = (int)P.slab, gz = P.Gz;
+    const int i0f = i0 + 2 * slab + 2 * gz + 2;   // loop node (0,0,0) of a flipped walk
+    const bool emit_a = active;
+    const bool emit_b = active && !merged;
+    // loop rows (a, b) = (0,0) (0,1) (0,2) (1,0) (1,1); u walks row starts
+#pragma unroll
+    for (int a = 0; a < 2; a++) {
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            if (9 * a + 3 * b > 13) continue;
+            if (b > 0) {
+#pragma unroll
+                for (int r = 0; r < 3; r++) { A.u[r] += A.s1h[r]; B.u[r] += B.s1h[r]; }
+            } else if (a > 0) {
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    A.u[r] += A.s0h[r] - 2.0f * A.s1h[r];
+                    B.u[r] += B.s0h[r] - 2.0f * B.s1h[r];
+                }
+            }
+            const float wab_a = A.wa[a] * A.wb[b], wab_b = B.wa[a] * B.wb[b];
+            float za[3], zb[3];
+#pragma unroll
+            for (int r = 0; r < 3; r++) { za[r] = A.u[r]; zb[r] = B.u[r]; }
+            const int off_ab = a * slab + b * gz;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const int j = 9 * a + 3 * b + c;
+                if (j > 13) continue;
+                if (c > 0) {
+#pragma unroll
+                    for (int r = 0; r < 3; r++) { za[r] += A.s2h[r]; zb[r] += B.s2h[r]; }
+                }
+                const float wa_ = wab_a * A.wc[c], wb_ = wab_b * B.wc[c];
+                float va[4] = {wa_ * A.m, wa_ * za[0], wa_ * za[1], wa_ * za[2]};
+                const float vb[4] = {wb_ * B.m, wb_ * zb[0], wb_ * zb[1], wb_ * zb[2]};
+                if (merged) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) va[q] += vb[q];
+                }
+                const int off = off_ab + c;
+                // the centre node (j == 13) belongs to the unflipped walk only
+                if (emit_a && !(j == 13 && second))
+                    atomicAdd(acc + (second ? i0f - off : i0 + off), make_float4(va[0], va[1], va[2], va[3]));
+                if (emit_b && j != 13)
+                    atomicAdd(acc + (first ? i0 + off : i0f - off), make_float4(vb[0], vb[1], vb[2], vb[3]));
+            }
+        }
+    }
+}
+
 // Shared-memory tile variant of the scatter. The block's particles (a
 // contiguous range of the cell-sorted order) span a small box of nodes; the
 // block accumulates the box with FP32 shared-memory atomics and adds each non-empty node to the grid once, as one
@@ -1142,7 +1269,8 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     if (SCATTER == 3 && p2g_scatter_tile_fx<128>(P, acc, reinterpret_cast<int*>(mixed_tile), tile_cap, active, inside,
                                                  base, fx, mass, mv, S, lane))
         return;
-    if (SCATTER == 4) p2g_scatter_pairs(P, acc, active, inside, base, fx, mass, mv, S, lane, wx);
+    if (SCATTER == 5) p2g_scatter_split(P, acc, active, inside, base, fx, mass, mv, S, lane, wx);
+    else if (SCATTER == 4) p2g_scatter_pairs(P, acc, active, inside, base, fx, mass, mv, S, lane, wx);
     else if (SCATTER == 1) p2g_scatter_mixed<false>(P, acc, active, inside, base, fx, mass, mv, S, lane);
     else p2g_scatter_mixed<true>(P, acc, active, inside, base, fx, mass, mv, S, lane);
 }

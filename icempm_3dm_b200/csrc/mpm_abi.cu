@@ -406,7 +406,8 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
             else if (sc == 0) FUSED_G(5, 0);
             else FUSED_G(5, 1);
         } else if (h->mixed_variant == 3) {
-            if (sc == 4) FUSED_G(8, 4);
+            if (sc == 5) FUSED_G(8, 5);
+            else if (sc == 4) FUSED_G(8, 4);
             else FUSED_G(8, 1);
         } else {
             if (sc == 4) FUSED_G(6, 4);
@@ -1106,7 +1107,7 @@ int mpm_testing_download_grid(mpm_handle* h, double* out, int which) {
 }
 
 int mpm_testing_set_p2g_variant(mpm_handle* h, int variant) {
-    if (!h || variant < 0 || variant > 9) return MPM_ERR_ARG;
+    if (!h || variant < 0 || variant > 10) return MPM_ERR_ARG;
     if (is_mixed(h)) {
         if (variant < 5) return MPM_ERR_ARG;
         h->mixed_scatter = variant - 5;

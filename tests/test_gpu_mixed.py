@@ -35,7 +35,7 @@ def test_upload_download_round_trip():
 
 
 # (p2g/scatter variant, g2p/gather variant) pairs of the fused kernel
-FUSED_VARIANTS = [(5, 2), (6, 2), (7, 2), (8, 2), (9, 2), (6, 3), (9, 3), (9, 4), (9, 5), (9, 6), (6, 6)]
+FUSED_VARIANTS = [(5, 2), (6, 2), (7, 2), (8, 2), (9, 2), (6, 3), (9, 3), (9, 4), (9, 5), (9, 6), (6, 6), (10, 5)]
 
 
 @pytest.mark.parametrize("scatter,gather", FUSED_VARIANTS)

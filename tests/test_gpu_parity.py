@@ -8,7 +8,7 @@ to ~1e-12 relative; the cell-key sort and the FP32 SVD are bit-exact.
 import numpy as np
 import pytest
 
-from icempm_3dm_b200 import MPMHandle, PRECISION_FP64, PRECISION_FP64_SVD64
+from icempm_3dm_b200 import MPMHandle, PRECISION_FP64, PRECISION_FP64_SVD64, PRECISION_MIXED
 from icempm_3dm_b200 import generator as gen
 from icempm_3dm_b200._lib import (BP00, FE00, IDX_JP_INV, IDX_P, IDX_Q, IDX_UTILITY, LIB, POSX, STATUS_DISABLED,
                                   VELX, check, dptr)
@@ -189,9 +189,10 @@ def test_fp64_svd_mode_matches_oracle_f64():
         assert ok, (r, rel)
 
 
+@pytest.mark.parametrize("precision", [PRECISION_FP64, PRECISION_MIXED])
 @pytest.mark.parametrize("axis,side,code", [(0, -1, 70), (1, -1, 71), (2, -1, 72), (0, 1, 73), (1, 1, 74),
                                              (2, 1, 75)])
-def test_out_of_grid_error_codes(axis, side, code):
+def test_out_of_grid_error_codes(axis, side, code, precision):
     prms, soa, _ = gen.small_block(n=500, seed=3)
     dims = [prms.GridXTotal + 2 * prms.GridHaloSize, prms.GridY, prms.GridZ]
     h_ = prms.cellsize
@@ -200,7 +201,7 @@ def test_out_of_grid_error_codes(axis, side, code):
     n = soa.shape[1]
     ref_grid, err = po.p2g(prms, soa, n)
     assert err == code
-    with MPMHandle(prms, n) as h:
+    with MPMHandle(prms, n, precision) as h:
         h.upload(soa)
         r = h.step(1, raise_on_error=False, want_forces=False)
         assert r == code
