@@ -6,4 +6,4 @@ reference-shaped host classes and the synthetic workload generator.
 """
 from ._lib import (LIB, LIB_PATH, MPMError, SimParams3D, PRECISION_FP64, PRECISION_MIXED,  # noqa: F401
                    PRECISION_FP64_SVD64, N_PTS_ARRAYS)
-from .simulation import MPMHandle, GPU_Implementation6, Model3D  # noqa: F401
+from .simulation import MPMHandle, GPU_Implementation6, Model3D, SnapshotManager  # noqa: F401

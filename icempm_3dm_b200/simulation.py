@@ -5,13 +5,19 @@
                        (simulation/gpu_implementation6.h:24-59) for one
                        partition: halo and point-transfer methods are no-ops
   Model3D              the substep loop of Model3D::Step (model_3d.cpp:24-112)
+  SnapshotManager      raw point-cloud loading, full snapshots and resume
+                       (snapshotmanager.cpp:20-113, :299-405) in the
+                       reference's HDF5 layout
 
 All device work runs in the CUDA library; nothing here computes physics.
 """
+import ctypes
+import os
+
 import numpy as np
 
+from . import snapshot as _snap
 from ._lib import (LIB, N_PTS_ARRAYS, PRECISION_FP64, MPMError, SimParams3D, check, dptr, uptr)
-import ctypes
 
 
 class MPMHandle:
@@ -242,13 +248,55 @@ class GPU_Implementation6:
 
 class Model3D:
     """Model3D::Step for one frame of UpdateEveryNthStep substeps, driving the
-    phase API exactly as the reference does (model_3d.cpp:24-112)."""
+    phase API exactly as the reference does (model_3d.cpp:24-112).
 
-    def __init__(self, prms, soa, cohesion=None, precision=PRECISION_FP64, device=0):
+    capacity: host/device capacity (default: the particle count); sort: run
+    RemoveDisabledAndSort (on the device) after the upload, as LoadRawPoints
+    and ReadSnapshot do."""
+
+    def __init__(self, prms, soa, cohesion=None, precision=PRECISION_FP64, device=0, capacity=None, sort=False):
         self.prms = prms.copy()
         self.gpu = GPU_Implementation6(self.prms, precision, device)
-        self.gpu.initialize(soa.shape[1])
+        self.gpu.initialize(soa.shape[1] if capacity is None else max(int(capacity), soa.shape[1]))
         self.gpu.transfer_ponts_to_device(soa, cohesion=cohesion)
+        if sort:
+            self.gpu.handle.sort()
+            self.gpu.hssoa = self.gpu.handle.download()
+        self.gpu.update_constants()
+
+    @classmethod
+    def from_config(cls, json_path, base_dir=None, precision=PRECISION_FP64, device=0):
+        """The CLI path (cli/main.cpp:54-58): SimParams3D::ParseFile, then
+        SnapshotManager::LoadRawPoints on InputRawPoints, resolved against
+        base_dir (default: the working directory, as the reference does)."""
+        p = SimParams3D()
+        raw = ctypes.create_string_buffer(4096)
+        check(LIB.mpm_params_parse_file(p, os.fspath(json_path).encode(), raw, len(raw)), "mpm_params_parse_file")
+        path = raw.value.decode()
+        if base_dir is not None and not os.path.isabs(path):
+            path = os.path.join(base_dir, path)
+        model = cls.__new__(cls)
+        model.prms = p
+        model.gpu = None
+        SnapshotManager(model).LoadRawPoints(path, precision, device)
+        return model
+
+    @classmethod
+    def from_snapshot(cls, path, partitions=0, precision=PRECISION_FP64, device=0):
+        """The CLI's --resume (cli/main.cpp:44-52): SnapshotManager::ReadSnapshot."""
+        model = cls.__new__(cls)
+        model.prms = SimParams3D()
+        model.gpu = None
+        SnapshotManager(model).ReadSnapshot(path, partitions, precision, device)
+        return model
+
+    def Reset(self):
+        """Model3D::Reset (model_3d.cpp:122-130)."""
+        self.prms.SimulationStep = 0
+        self.prms.SimulationTime = 0.0
+
+    def Prepare(self):
+        """Model3D::Prepare (model_3d.cpp:132-137)."""
         self.gpu.update_constants()
 
     def Step(self, substeps=None):
@@ -275,3 +323,55 @@ class Model3D:
         p.SimulationStep += count
         self.gpu.transfer_from_device()
         return p.SimulationTime < p.SimulationEndTime
+
+
+class SnapshotManager:
+    """Method-for-method mirror of the reference class (snapshotmanager.h:15-42)
+    for the raw point-cloud loader, the full snapshot and resume; the files
+    are the reference's (see icempm_3dm_b200.snapshot)."""
+
+    def __init__(self, model):
+        self.model = model
+        self.previous_frame_exists = False
+
+    def LoadRawPoints(self, fileName, precision=None, device=0):
+        """snapshotmanager.cpp:20-113: read and place the points, allocate
+        (capacity n * (1 + ExtraSpaceForIncomingPoints)), upload, sort on the
+        device, Reset, Prepare."""
+        m = self.model
+        p, soa, capacity = _snap.load_raw_points(fileName, m.prms)
+        prec = precision if precision is not None else (m.gpu.precision if m.gpu else PRECISION_FP64)
+        dev = m.gpu.device if m.gpu else device
+        if m.gpu is not None and m.gpu.handle is not None:
+            m.gpu.handle.close()
+        Model3D.__init__(m, p, soa, precision=prec, device=dev, capacity=capacity, sort=True)
+        m.Reset()
+        m.Prepare()
+        self.previous_frame_exists = False
+
+    def SaveSnapshot(self, outputDirectory, frame, compress=False):
+        """snapshotmanager.cpp:299-340: d<frame>.h5 from the current host SoA
+        (downloaded) at the handle's capacity."""
+        m = self.model
+        g = m.gpu
+        g.transfer_from_device()
+        size = g.hssoa.shape[1]
+        buf = np.zeros((N_PTS_ARRAYS, g.handle.capacity), dtype=np.float64)
+        buf[:, :size] = g.hssoa
+        return _snap.save_snapshot(outputDirectory, frame, m.prms, buf, size, g.indenter_sensor_total, compress)
+
+    def ReadSnapshot(self, fileName, partitions=0, precision=None, device=0):
+        """snapshotmanager.cpp:346-405: parameters from the attributes, the
+        points (sorted on the device when SimulationStep != 0), Prepare, and
+        the indenter accumulator."""
+        m = self.model
+        p, hssoa, size, ind = _snap.read_snapshot(fileName, partitions)
+        prec = precision if precision is not None else (m.gpu.precision if m.gpu else PRECISION_FP64)
+        dev = m.gpu.device if m.gpu else device
+        if m.gpu is not None and m.gpu.handle is not None:
+            m.gpu.handle.close()
+        Model3D.__init__(m, p, np.ascontiguousarray(hssoa[:, :size]), precision=prec, device=dev,
+                         capacity=hssoa.shape[1], sort=p.SimulationStep != 0)
+        m.Prepare()
+        m.gpu.indenter_sensor_total = ind
+        self.previous_frame_exists = False
