@@ -117,6 +117,8 @@ ENTRY_POINTS = [
     ("mpm_download_ids", ctypes.c_int, [_hp, _up, _up]),
     ("mpm_sort", ctypes.c_int, [_hp]),
     ("mpm_set_sort_interval", ctypes.c_int, [_hp, ctypes.c_int]),
+    ("mpm_frame_records", ctypes.c_int, [_hp, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, _up, ctypes.c_void_p, _up,
+                                         ctypes.c_void_p, _up, ctypes.c_void_p, _up]),
     ("mpm_reset_grid", ctypes.c_int, [_hp]),
     ("mpm_p2g", ctypes.c_int, [_hp]),
     ("mpm_update_nodes", ctypes.c_int, [_hp, ctypes.c_double, ctypes.c_double]),

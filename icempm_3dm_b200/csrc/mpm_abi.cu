@@ -26,6 +26,7 @@
 #include "kernels_mixed.cuh"
 #include "adjoint_f64.cuh"
 #include "sort.cuh"
+#include "frames.cuh"
 
 using namespace icempm;
 
@@ -123,6 +124,15 @@ struct mpm_handle {
     int fx_tile_cap = 3072;           // nodes of the fixed-point tile (x 32 B)
     float* chunk_bound = nullptr;     // per-chunk |contribution| bound of the fixed-point P2G
     int chunk_bound_cap = 0;
+
+    // animation-frame records (mpm_frame_records), allocated on first use
+    float* fr_f = nullptr;            // visual state: pos 3, vel 3, Jp_inv rows x pitch
+    unsigned char* fr_status = nullptr;
+    int* fr_last = nullptr;           // frame of each visual point's last position refresh
+    int* fr_i = nullptr;              // keep, rank, 3 flags, 3 offsets: 8 x (pitch + 1)
+    unsigned char* fr_rec = nullptr;  // records: 44 bytes x pitch
+    std::vector<int*> fr_scan_levels;
+    bool fr_ready = false;            // a full frame has built the visual state
     cudaError_t last_cuda = cudaSuccess;
 };
 
@@ -220,6 +230,9 @@ void free_all(mpm_handle* h) {
     cudaFree(h->adj_A); cudaFree(h->adj_cgrad); cudaFree(h->adj_Egrad); cudaFree(h->adj_g7); cudaFree(h->adj_gb7);
     for (int* p : h->scan_levels) cudaFree(p);
     h->scan_levels.clear();
+    cudaFree(h->fr_f); cudaFree(h->fr_status); cudaFree(h->fr_last); cudaFree(h->fr_i); cudaFree(h->fr_rec);
+    for (int* p : h->fr_scan_levels) cudaFree(p);
+    h->fr_scan_levels.clear();
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
 }
 
@@ -507,14 +520,18 @@ int ensure_sort_scratch(mpm_handle* h) {
     return MPM_OK;
 }
 
-int exclusive_scan(mpm_handle* h, const int* in, int* out, int n, size_t level) {
+// Exclusive scan of n ints; `levels` holds the tile sums and their scans of
+// each level, sized for at least n (default: the sort's, sized for the cells).
+int exclusive_scan(mpm_handle* h, const int* in, int* out, int n, size_t level,
+                   const std::vector<int*>* levels = nullptr) {
+    const std::vector<int*>& lv = levels ? *levels : h->scan_levels;
     const int tiles = (n + kScanTile - 1) / kScanTile;
-    int* sums = tiles > 1 ? h->scan_levels[2 * level] : nullptr;
+    int* sums = tiles > 1 ? lv[2 * level] : nullptr;
     k_scan_tiles<<<tiles, kScanBlock, 0, h->stream>>>(in, out, n, sums);
     CK_LAUNCH(h, "scan tiles");
     if (tiles > 1) {
-        int* scanned = h->scan_levels[2 * level + 1];
-        int r = exclusive_scan(h, sums, scanned, tiles, level + 1);
+        int* scanned = lv[2 * level + 1];
+        int r = exclusive_scan(h, sums, scanned, tiles, level + 1, levels);
         if (r) return r;
         k_scan_add<<<blocks_for(n, 256), 256, 0, h->stream>>>(out, n, scanned);
         CK_LAUNCH(h, "scan add");
@@ -789,6 +806,118 @@ int mpm_set_sort_interval(mpm_handle* h, int k) {
     if (!h || k < 0) return MPM_ERR_ARG;
     h->sort_interval = k;
     return MPM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+int ensure_frame_scratch(mpm_handle* h) {
+    if (h->fr_f) return MPM_OK;
+    const size_t p = h->pitch;
+    CK(h, cudaMalloc(&h->fr_f, sizeof(float) * 7 * p));
+    CK(h, cudaMalloc(&h->fr_status, p));
+    CK(h, cudaMalloc(&h->fr_last, sizeof(int) * p));
+    CK(h, cudaMalloc(&h->fr_i, sizeof(int) * 8 * (p + 1)));
+    CK(h, cudaMalloc(&h->fr_rec, (sizeof(UpdPosRec) + sizeof(UpdJpRec) + sizeof(UpdStatusRec)) * p));
+    long long m = (long long)p + 1;
+    while (m > kScanTile) {
+        m = (m + kScanTile - 1) / kScanTile;
+        int* sums = nullptr;
+        int* scanned = nullptr;
+        CK(h, cudaMalloc(&sums, sizeof(int) * m));
+        CK(h, cudaMalloc(&scanned, sizeof(int) * m));
+        h->fr_scan_levels.push_back(sums);
+        h->fr_scan_levels.push_back(scanned);
+    }
+    return MPM_OK;
+}
+
+template <class Pts>
+int frame_records(mpm_handle* h, Pts pts, int frame, int full, mpm_visual_point* points, unsigned* n_points,
+                  mpm_update_pos* upd_pos, unsigned* n_pos, mpm_update_jp* upd_jp, unsigned* n_jp,
+                  mpm_update_status* upd_status, unsigned* n_status) {
+    const int n = (int)h->n;
+    const size_t p = h->pitch, m = p + 1;
+    int* keep = h->fr_i;
+    int* rank = keep + m;
+    int* flags = rank + m;
+    int* offs = flags + 3 * m;
+    FrameVis v{h->fr_f, h->fr_f + 3 * p, h->fr_f + 6 * p, h->fr_status, h->fr_last, p};
+    const unsigned nb = blocks_for(n, 256);
+    CK(h, cudaMemsetAsync(keep + n, 0, sizeof(int), h->stream));
+    if (n) {
+        k_frame_keep<<<nb, 256, 0, h->stream>>>(pts, n, keep);
+        CK_LAUNCH(h, "frame keep");
+    }
+    int r = exclusive_scan(h, keep, rank, n + 1, 0, &h->fr_scan_levels);
+    if (r) return r;
+    if (full) {
+        auto* rec = reinterpret_cast<VisualPointRec*>(h->fr_rec);
+        if (n) {
+            k_frame_full<<<nb, 256, 0, h->stream>>>(pts, n, rank, v, frame, rec);
+            CK_LAUNCH(h, "frame full");
+        }
+        int cnt = 0;
+        CK(h, cudaMemcpyAsync(&cnt, rank + n, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        if (cnt) CK(h, cudaMemcpyAsync(points, rec, sizeof(VisualPointRec) * cnt, cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        *n_points = (unsigned)cnt;
+        h->fr_ready = true;
+        return MPM_OK;
+    }
+    for (int k = 0; k < 3; k++) CK(h, cudaMemsetAsync(flags + k * m + n, 0, sizeof(int), h->stream));
+    if (n) {
+        k_frame_flags<<<nb, 256, 0, h->stream>>>(pts, n, rank, v, frame, h->prms.InitialTimeStep,
+                                                 h->prms.UpdateEveryNthStep, h->prms.animation_threshold_pos,
+                                                 flags, m);
+        CK_LAUNCH(h, "frame flags");
+    }
+    for (int k = 0; k < 3; k++) {
+        r = exclusive_scan(h, flags + k * m, offs + k * m, n + 1, 0, &h->fr_scan_levels);
+        if (r) return r;
+    }
+    auto* upv = reinterpret_cast<UpdPosRec*>(h->fr_rec);
+    auto* ujp = reinterpret_cast<UpdJpRec*>(h->fr_rec + sizeof(UpdPosRec) * p);
+    auto* ust = reinterpret_cast<UpdStatusRec*>(h->fr_rec + (sizeof(UpdPosRec) + sizeof(UpdJpRec)) * p);
+    if (n) {
+        k_frame_emit<<<nb, 256, 0, h->stream>>>(pts, n, rank, flags, offs, m, upv, ujp, ust);
+        CK_LAUNCH(h, "frame emit");
+    }
+    int cnt[3] = {0, 0, 0};
+    for (int k = 0; k < 3; k++)
+        CK(h, cudaMemcpyAsync(cnt + k, offs + k * m + n, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (cnt[0]) CK(h, cudaMemcpyAsync(upd_pos, upv, sizeof(UpdPosRec) * cnt[0], cudaMemcpyDeviceToHost, h->stream));
+    if (cnt[1]) CK(h, cudaMemcpyAsync(upd_jp, ujp, sizeof(UpdJpRec) * cnt[1], cudaMemcpyDeviceToHost, h->stream));
+    if (cnt[2])
+        CK(h, cudaMemcpyAsync(upd_status, ust, sizeof(UpdStatusRec) * cnt[2], cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    *n_pos = (unsigned)cnt[0];
+    *n_jp = (unsigned)cnt[1];
+    *n_status = (unsigned)cnt[2];
+    return MPM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mpm_frame_records(mpm_handle* h, int frame, int full, mpm_visual_point* points, unsigned* n_points,
+                      mpm_update_pos* upd_pos, unsigned* n_pos, mpm_update_jp* upd_jp, unsigned* n_jp,
+                      mpm_update_status* upd_status, unsigned* n_status) {
+    if (!h) return MPM_ERR_ARG;
+    if (full ? (!points || !n_points) : (!upd_pos || !n_pos || !upd_jp || !n_jp || !upd_status || !n_status))
+        return MPM_ERR_ARG;
+    if (!h->uploaded || (!full && !h->fr_ready)) return MPM_ERR_STATE;
+    int r = ensure_frame_scratch(h);
+    if (r) return r;
+    if (is_mixed(h))
+        return frame_records(h, FramePointsMixed{mixed_state(h), h->prms.cellsize}, frame, full, points, n_points,
+                             upd_pos, n_pos, upd_jp, n_jp, upd_status, n_status);
+    return frame_records(h, FramePointsF64{h->pts, h->pitch}, frame, full, points, n_points, upd_pos, n_pos, upd_jp,
+                         n_jp, upd_status, n_status);
 }
 
 int mpm_reset_grid(mpm_handle* h) {

@@ -9,8 +9,9 @@ properties, simulation/snapshotmanager.cpp:20-45 and :299-405):
 - the root group as a symbol table (version 1 B-tree of type 0, local heap,
   symbol table nodes), datasets directly under it;
 - version 1 object headers, with continuation blocks;
-- dataspace (versions 1, 2), datatype (version 1: fixed-point and IEEE float,
-  little- or big-endian), fill value (version 2), data layout (version 3:
+- dataspace (versions 1, 2), datatype (fixed-point and IEEE float, little-
+  or big-endian; compounds of them, as the animation frames' records use),
+  fill value (version 2), data layout (version 3:
   compact, contiguous, chunked; versions 1 and 2 read), filter pipeline
   (versions 1, 2: deflate, shuffle, Fletcher-32), attributes (versions 1-3);
 - chunk indexes as version 1 B-trees of type 1, any depth.
@@ -309,6 +310,7 @@ def _parse_dataspace(d):
 
 
 def _parse_datatype(d):
+    """(numpy dtype, bytes used) of a datatype message."""
     cls, ver = d[0] & 0x0F, d[0] >> 4
     bits = d[1] | (d[2] << 8) | (d[3] << 16)
     size = int.from_bytes(d[4:8], "little")
@@ -324,6 +326,27 @@ def _parse_datatype(d):
         if size not in (4, 8):
             raise H5Error(f"floating-point size {size}")
         return np.dtype(f"{order}f{size}"), 20
+    if cls == 6:
+        names, formats, offsets = [], [], []
+        p = 8
+        for _ in range(bits & 0xFFFF):
+            end = d.index(b"\0", p)
+            names.append(d[p:end].decode())
+            p = p + _pad8(end - p + 1) if ver < 3 else end + 1
+            if ver < 3:
+                off, p = int.from_bytes(d[p:p + 4], "little"), p + 4
+            else:
+                w = 1 if size < 1 << 8 else 2 if size < 1 << 16 else 3 if size < 1 << 24 else 4
+                off, p = int.from_bytes(d[p:p + w], "little"), p + w
+            if ver == 1:
+                if d[p] != 0:
+                    raise H5Error("compound members with array dimensions are not read")
+                p += 28
+            sub, used = _parse_datatype(d[p:])
+            p += used
+            formats.append(sub)
+            offsets.append(off)
+        return np.dtype({"names": names, "formats": formats, "offsets": offsets, "itemsize": size}), p
     raise H5Error(f"datatype class {cls} is not read")
 
 
@@ -405,8 +428,22 @@ def _unfilter(raw, filters, mask, elem):
 # ------------------------------------------------------------------ writing
 
 def _datatype_bytes(dt):
-    """Version-1 datatype message for a native numeric type (unpadded)."""
+    """Version-1 datatype message (unpadded) for a native numeric type, or a
+    compound of them (class 6: per member the name padded to 8 bytes, the
+    byte offset, the version-1 dimension fields, all zero, and the member's
+    datatype)."""
     dt = np.dtype(dt)
+    if dt.names is not None:
+        body = b""
+        for name in dt.names:
+            sub, off = dt.fields[name][:2]
+            if sub.names is not None or sub.shape:
+                raise H5Error("nested or array compound members are not written")
+            nm = name.encode() + b"\0"
+            body += nm + b"\0" * (_pad8(len(nm)) - len(nm))
+            body += struct.pack("<I", off) + b"\0" * 28 + _datatype_bytes(sub)
+        n = len(dt.names)
+        return bytes([0x16, n & 0xFF, n >> 8, 0]) + struct.pack("<I", dt.itemsize) + body
     if dt.byteorder == ">":
         raise H5Error("big-endian data is not written")
     if dt.kind in "iu":

@@ -78,6 +78,22 @@ class MPMHandle:
     def sort(self):
         return check(LIB.mpm_sort(self._h), "mpm_sort")
 
+    def frame_records(self, frame, full):
+        """mpm_frame_records: the VisualPoint records (full) or the
+        (UpdatePos, UpdateJp, UpdateStatus) records of this frame."""
+        cap = max(self.count(), 1)
+        if full:
+            pts = np.zeros(cap, dtype=_snap.VISUAL_POINT)
+            n = ctypes.c_uint(0)
+            check(LIB.mpm_frame_records(self._h, frame, 1, pts.ctypes.data, ctypes.byref(n), None, None, None, None,
+                                        None, None), "mpm_frame_records")
+            return pts[:n.value]
+        pv, jp, st = (np.zeros(cap, dtype=d) for d in (_snap.UPDATE_POS, _snap.UPDATE_JP, _snap.UPDATE_STATUS))
+        c = [ctypes.c_uint(0) for _ in range(3)]
+        check(LIB.mpm_frame_records(self._h, frame, 0, None, None, pv.ctypes.data, ctypes.byref(c[0]), jp.ctypes.data,
+                                    ctypes.byref(c[1]), st.ctypes.data, ctypes.byref(c[2])), "mpm_frame_records")
+        return pv[:c[0].value], jp[:c[1].value], st[:c[2].value]
+
     def set_sort_interval(self, k):
         check(LIB.mpm_set_sort_interval(self._h, k), "mpm_set_sort_interval")
 
@@ -359,6 +375,26 @@ class SnapshotManager:
         buf = np.zeros((N_PTS_ARRAYS, g.handle.capacity), dtype=np.float64)
         buf[:, :size] = g.hssoa
         return _snap.save_snapshot(outputDirectory, frame, m.prms, buf, size, g.indenter_sensor_total, compress)
+
+    def SaveFrame(self, outputDirectory, frame):
+        """snapshotmanager.cpp:116-293: v<frame>.h5, a full frame when no
+        previous frame exists, else the changed points (mpm_frame_records).
+        Uses the sensors and force of the last transfer_from_device (the
+        end of Model3D.Step)."""
+        m = self.model
+        g = m.gpu
+        if g.indenter_sensor_total is None:
+            g.transfer_from_device()
+        prev = self.previous_frame_exists
+        if not prev:
+            recs = {"points": g.handle.frame_records(frame, True)}
+        else:
+            pv, jp, st = g.handle.frame_records(frame, False)
+            recs = {"upd_pos": pv, "upd_jp": jp, "upd_status": st}
+        path = _snap.save_frame(outputDirectory, frame, m.prms, g.indenter_sensor_total, g.indenter_force, prev,
+                                **recs)
+        self.previous_frame_exists = True
+        return path
 
     def ReadSnapshot(self, fileName, partitions=0, precision=None, device=0):
         """snapshotmanager.cpp:346-405: parameters from the attributes, the

@@ -1,11 +1,11 @@
 """SnapshotManager of the reference (simulation/snapshotmanager.{h,cpp}) on
 the HDF5 codec of h5io: the raw point-cloud loader, the full snapshot
-d%05d.h5 (checkpoint) and resume from it, plus the parameter attributes of
-SimParams3D (parameters_sim_3d.cpp:178-282).
+d%05d.h5 (checkpoint) and resume from it, the animation frames v%05d.h5,
+plus the parameter attributes of SimParams3D (parameters_sim_3d.cpp:178-282).
 
-Files are interchangeable with the reference's: the same dataset names,
-shapes, element types, chunking, deflate level and attribute names/types in
-the same order. The host SoA is the reference's HostSideSOA buffer: 28 rows
+The files carry the reference's dataset names, shapes, element types,
+chunking, deflate levels and attribute names and types, in the reference's
+order. The host SoA is the reference's HostSideSOA buffer: 28 rows
 of `capacity` doubles (row k at offset k * capacity), `size` of them in use.
 
 RemoveDisabledAndSort, which LoadRawPoints and ReadSnapshot run on the host
@@ -14,6 +14,7 @@ cell-key order) when the model uploads the points.
 """
 import math
 import os
+import time
 
 import numpy as np
 
@@ -82,8 +83,9 @@ def load_raw_points(path, prms):
     """SnapshotManager::LoadRawPoints (snapshotmanager.cpp:20-113) up to the
     upload. Reads llGrainIDs (into the utility row, as raw uint64), x, y, z
     and the 'volume' attribute; places the block as the reference does (x and
-    z centred in the grid, lowest point at y = 2h; SetupType 2 marks the
-    points outside the centred cutout as liquid before the offset); sets
+    z shifted by (grid length - block length) / 2, y so that the lowest
+    point is 2h above the floor; SetupType 2 marks the points outside the
+    cutout centred in x and z at the block's top as liquid before the shift); sets
     F = I, Jp_inv = 1 (HostSideSOA::InitializeBlock), the indenter start and
     ParticleVolume = Volume / n. Returns (prms, soa, capacity): a copy of
     prms, the (28, n) SoA in file order (the cell-key sort follows on the
@@ -193,3 +195,62 @@ def read_snapshot(path, partitions=0):
             raise ValueError("Points does not hold capacity * 28 values")
         ind = f.read("Indenter")
     return p, pts.reshape(N_PTS_ARRAYS, capacity), size, ind
+
+
+# Record types of the animation frames (converter/visualpoint.cpp:12-41),
+# with the reference's member names, offsets and sizes.
+VISUAL_POINT = np.dtype({"names": ["px", "py", "pz", "vx", "vy", "vz", "Jp_inv", "status"],
+                         "formats": ["<f4"] * 7 + ["u1"], "offsets": [0, 4, 8, 12, 16, 20, 24, 28], "itemsize": 32})
+UPDATE_POS = np.dtype({"names": ["idx", "px", "py", "pz", "vx", "vy", "vz"], "formats": ["<i4"] + ["<f4"] * 6,
+                       "offsets": [0, 4, 8, 12, 16, 20, 24], "itemsize": 28})
+UPDATE_JP = np.dtype({"names": ["idx", "Jp_inv"], "formats": ["<i4", "<f4"], "offsets": [0, 4], "itemsize": 8})
+UPDATE_STATUS = np.dtype({"names": ["idx", "status"], "formats": ["<i4", "u1"], "offsets": [0, 4], "itemsize": 8})
+
+
+def frame_path(output_directory, frame):
+    return os.path.join(output_directory, f"v{frame:05d}.h5")
+
+
+def save_frame(output_directory, frame, prms, indenter_sensor_total, indenter_force, previous_frame_exists,
+               points=None, upd_pos=None, upd_jp=None, upd_status=None, timestamp=None):
+    """SnapshotManager::SaveFrame's file (snapshotmanager.cpp:116-293):
+    v<frame>.h5 with 'Indenter' (chunks of min(10000, size), deflate 5) and
+    its attributes indenter_total_x/y/z, partial_frame (uint8), the parameter
+    attributes and timestamp (uint64, seconds since the epoch); then either
+    'VisualPoints' (a full frame, when no previous frame exists; chunks of
+    min(2^20, count)) or the non-empty ones of 'UpdatePos', 'UpdateStatus',
+    'UpdateJp' (chunks of min(65536, count)), all deflate 5. The records are
+    those of mpm_frame_records. Returns the path."""
+    os.makedirs(output_directory, exist_ok=True)
+    ind = np.ascontiguousarray(indenter_sensor_total, dtype=np.float64).reshape(-1)
+    if ind.size != 3 * prms.IndenterSubdivisions * prms.GridZ:
+        raise ValueError("indenter sensor array does not match the parameters")
+    f = np.asarray(indenter_force, dtype=np.float64).reshape(3)
+    attrs = {"indenter_total_x": F64(f[0]), "indenter_total_y": F64(f[1]), "indenter_total_z": F64(f[2]),
+             "partial_frame": U8(1 if previous_frame_exists else 0)}
+    attrs.update(params_as_attributes(prms))
+    attrs["timestamp"] = U64(int(time.time()) if timestamp is None else timestamp)
+    path = frame_path(output_directory, frame)
+    with H5Writer(path) as w:
+        w.create_dataset("Indenter", ind, chunks=(min(10000, ind.size),), deflate=5, attrs=attrs)
+        if not previous_frame_exists:
+            pts = np.asarray(points, dtype=VISUAL_POINT)
+            w.create_dataset("VisualPoints", pts, chunks=(max(1, min(1024 * 1024, pts.size)),), deflate=5)
+        else:
+            for name, recs, dt in (("UpdatePos", upd_pos, UPDATE_POS), ("UpdateStatus", upd_status, UPDATE_STATUS),
+                                   ("UpdateJp", upd_jp, UPDATE_JP)):
+                recs = np.asarray(recs, dtype=dt)
+                if recs.size:
+                    w.create_dataset(name, recs, chunks=(min(1024 * 64, recs.size),), deflate=5)
+    return path
+
+
+def read_frame(path):
+    """The contents of a v<frame>.h5 file: {'attrs': Indenter's attributes,
+    'Indenter': array, and whichever of 'VisualPoints', 'UpdatePos',
+    'UpdateStatus', 'UpdateJp' it holds}."""
+    with H5File(path) as f:
+        out = {"attrs": f.attrs("Indenter")}
+        for k in f.keys():
+            out[k] = f.read(k)
+    return out

@@ -129,6 +129,38 @@ int  mpm_sort(mpm_handle* h);
  * default, as with one partition the reference never re-sorts). */
 int  mpm_set_sort_interval(mpm_handle* h, int k);
 
+/* ------------------------------------------------ animation-frame records */
+
+/* The records of SnapshotManager::SaveFrame (snapshotmanager.cpp:116-293) in
+ * the reference's memory layout (converter/visualpoint.h:7-11,
+ * snapshotmanager.h:30-36): VisualPoint, std::pair<int, std::array<float,6>>,
+ * std::pair<int, float>, std::pair<int, uint8_t>. */
+typedef struct { float pos[3], vel[3], Jp_inv; uint8_t status, pad[3]; } mpm_visual_point;   /* 32 bytes */
+typedef struct { int32_t idx; float pos[3], vel[3]; } mpm_update_pos;                          /* 28 bytes */
+typedef struct { int32_t idx; float Jp_inv; } mpm_update_jp;                                   /*  8 bytes */
+typedef struct { int32_t idx; uint8_t status, pad[3]; } mpm_update_status;                     /*  8 bytes */
+
+/* SaveFrame's change detection, on the device. The visual index of a
+ * particle is its rank among the non-disabled particles in the handle's
+ * current order; status byte = partition id (bits 24-31 of the status word)
+ * | 0x80 if crushed; positions, velocities and Jp_inv are cast to float.
+ * full != 0 (SaveFrame without a previous frame): keeps every particle as
+ * the visual state, with `frame` as its last position refresh, and copies
+ * the VisualPoint records to `points` (*n_points of them; room for the
+ * particle count). full == 0 (needs a full frame first, else
+ * MPM_ERR_STATE): for each particle, in order,
+ *   |pos - (vpos + vvel * (float)(dt * (frame - last) * UpdateEveryNthStep))|
+ *   > animation_threshold_pos -> an UpdatePos record, last = frame;
+ *   |vJp_inv - Jp_inv| > 1e-2  -> an UpdateJp record;
+ *   status byte changed        -> an UpdateStatus record;
+ * each output holds room for the particle count, the counts are returned.
+ * As in the reference (which updates a copy of visual_state[count]), a
+ * partial frame changes only `last`; the kept positions, velocities,
+ * Jp_inv and status bytes stay those of the last full frame. */
+int  mpm_frame_records(mpm_handle* h, int frame, int full, mpm_visual_point* points, unsigned* n_points,
+                       mpm_update_pos* upd_pos, unsigned* n_pos, mpm_update_jp* upd_jp, unsigned* n_jp,
+                       mpm_update_status* upd_status, unsigned* n_status);
+
 /* ------------------------------------------ substep phases (one partition) */
 
 /* GPU_Implementation6::reset_grid (gpu_implementation6.cpp:18-29). */

@@ -123,3 +123,39 @@ def test_partitions_override_and_missing_files(tmp_path):
         snapshot.load_raw_points(str(tmp_path / "nope.h5"), p)
     with pytest.raises(ValueError):
         snapshot.save_snapshot(str(tmp_path), 1, p, hs, 10, np.zeros(5))
+
+
+def test_frame_file_layout(tmp_path):
+    """SaveFrame's file: Indenter (chunks of min(10000, size), deflate 5) with
+    its attributes in order, VisualPoints or the non-empty delta datasets as
+    compounds with the reference's member names, offsets and sizes."""
+    from icempm_3dm_b200 import h5io
+    p = _params()
+    ind = np.arange(3 * p.IndenterSubdivisions * p.GridZ, dtype=np.float64)
+    pts = np.zeros(50, dtype=snapshot.VISUAL_POINT)
+    pts["px"] = np.arange(50)
+    pts["status"] = 0x83
+    full = snapshot.save_frame(str(tmp_path), 7, p, ind, [1.0, 2.0, 3.0], False, points=pts, timestamp=1234)
+    pv = np.zeros(4, dtype=snapshot.UPDATE_POS)
+    pv["idx"] = [1, 5, 9, 11]
+    jp = np.zeros(0, dtype=snapshot.UPDATE_JP)
+    st = np.zeros(2, dtype=snapshot.UPDATE_STATUS)
+    st["status"] = [0x80, 0x01]
+    part = snapshot.save_frame(str(tmp_path), 8, p, ind, [0.0, 0.0, 0.0], True, upd_pos=pv, upd_jp=jp, upd_status=st)
+    assert full.endswith("v00007.h5") and part.endswith("v00008.h5")
+    f = snapshot.read_frame(full)
+    assert list(f["attrs"])[:4] == ["indenter_total_x", "indenter_total_y", "indenter_total_z", "partial_frame"]
+    assert list(f["attrs"])[-1] == "timestamp" and f["attrs"]["timestamp"] == 1234
+    assert f["attrs"]["timestamp"].dtype == np.uint64 and f["attrs"]["partial_frame"].dtype == np.uint8
+    assert f["attrs"]["indenter_total_z"] == 3.0 and f["attrs"]["partial_frame"] == 0
+    assert np.array_equal(f["Indenter"], ind) and np.array_equal(f["VisualPoints"], pts)
+    g = snapshot.read_frame(part)
+    assert g["attrs"]["partial_frame"] == 1
+    assert set(g) == {"attrs", "Indenter", "UpdatePos", "UpdateStatus"}      # empty UpdateJp is not written
+    assert np.array_equal(g["UpdatePos"], pv) and np.array_equal(g["UpdateStatus"], st)
+    assert snapshot.UPDATE_POS.itemsize == 28 and snapshot.UPDATE_STATUS.itemsize == 8
+    with h5io.H5File(full) as h:
+        lay = [h5io._parse_layout(d) for t, fl, d in h._messages(h._datasets["Indenter"]) if t == 0x08][0]
+        filt = [h5io._parse_filters(d) for t, fl, d in h._messages(h._datasets["VisualPoints"]) if t == 0x0B][0]
+    assert lay[0] == "chunked" and lay[2] == (min(10000, ind.size), 8)
+    assert filt == [(1, 1, (5,))]
