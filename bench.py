@@ -356,13 +356,16 @@ def run_ours(args):
 
 
 def run_adjoint(args):
-    """One JSON line: the adjoint of the FP64 step (mpm_adjoint_forward with a
-    checkpoint every --ckpt-every substeps, then mpm_adjoint_backward) on the
-    calibration workload (default calib500k: 500,000 particles, 200 substeps),
-    as particle-steps/s of forward + reverse together, beside the plain FP64
-    step on the same block. CUDA events on the handle's stream."""
+    """One JSON line: the adjoint (mpm_adjoint_forward with a checkpoint every
+    --ckpt-every substeps, then mpm_adjoint_backward) on the calibration
+    workload (default calib500k: 500,000 particles, 200 substeps), as
+    particle-steps/s of forward + reverse together, beside the plain step of
+    the same precision on the same block. --precision mixed (the default)
+    runs the forward in mixed precision, with FP64 checkpoints and the FP64
+    recompute in the reverse sweep; fp64 runs it in FP64 with the FP64 SVD.
+    CUDA events on the handle's stream."""
     import torch
-    from icempm_3dm_b200 import MPMHandle, PRECISION_FP64_SVD64
+    from icempm_3dm_b200 import MPMHandle, PRECISION_FP64_SVD64, PRECISION_MIXED
     from icempm_3dm_b200 import generator as gen
     torch.cuda.set_device(0)
     cfg = gen.CONFIGS[args.workload if args.workload != "block8m" else "calib500k"]
@@ -372,7 +375,8 @@ def run_adjoint(args):
     n = soa.shape[1]
     steps = args.steps if args.steps != 1500 else cfg.steps
     stream = torch.cuda.Stream()
-    h = MPMHandle(prms, n, PRECISION_FP64_SVD64)
+    prec = PRECISION_MIXED if args.precision == "mixed" else PRECISION_FP64_SVD64
+    h = MPMHandle(prms, n, prec)
     h.set_stream(stream.cuda_stream)
     rng = np.random.default_rng(0)
     w = rng.standard_normal((steps, 3))
@@ -397,8 +401,9 @@ def run_adjoint(args):
     out = {"metric": "adjoint particle-steps/s (forward with checkpoints + reverse)",
            "value": n * steps / (t_adj * 1e-3), "unit": "particle-steps/s", "n_gpus": 1, "steps": steps,
            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": cfg.name, "particles": n, "ckpt_every": args.ckpt_every},
-           "ms_adjoint": t_adj, "ms_plain_fp64_forward": t_fwd, "adjoint_over_forward": t_adj / t_fwd}
+           "config": {"workload": cfg.name, "particles": n, "ckpt_every": args.ckpt_every,
+                      "forward_precision": args.precision},
+           "ms_adjoint": t_adj, "ms_plain_forward": t_fwd, "adjoint_over_forward": t_adj / t_fwd}
     print(json.dumps(out), flush=True)
     return 0
 

@@ -1,14 +1,18 @@
-"""torch.autograd wrapper of the hand-written adjoint of the FP64 step.
+"""torch.autograd wrapper of the hand-written adjoint of the step.
 
     hist = indenter_force_history(state, cohesion, youngs_modulus, prms, nsteps)
     loss = ((hist - measured) ** 2).sum()
     loss.backward()        # cohesion.grad, youngs_modulus.grad, state.grad
 
 The forward runs mpm_adjoint_forward (nsteps substeps of Model3D::Step,
-model_3d.cpp:35-51, with FP64 state and FP64 SVD, a device checkpoint every
-ckpt_every substeps); the backward runs mpm_adjoint_backward (each segment
-recomputed from its checkpoint, then reverse G2P, reverse grid update,
-reverse P2G as a gather) with grad_output as dL/d(force history).
+model_3d.cpp:35-51, a device checkpoint every ckpt_every substeps) in FP64
+with the FP64 SVD, or with precision=PRECISION_MIXED in mixed precision (the
+checkpoints are then FP64 copies of the mixed state); the backward runs
+mpm_adjoint_backward (each segment recomputed in FP64 from its checkpoint,
+then reverse G2P, reverse grid update, reverse P2G as a gather) with
+grad_output as dL/d(force history). With a mixed forward the gradient is
+that of the FP64 step along the mixed trajectory, restarted at every
+checkpoint.
 
 Inputs are float64 tensors on any device (they are staged through host
 memory to the C-ABI, which takes host buffers):
@@ -43,13 +47,13 @@ def _params_with_E(prms, E):
 
 class IndenterForceHistory(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, state, cohesion, youngs_modulus, prms, nsteps, ckpt_every, device):
+    def forward(ctx, state, cohesion, youngs_modulus, prms, nsteps, ckpt_every, device, precision):
         if state.dtype != torch.float64 or cohesion.dtype != torch.float64:
             raise TypeError("state and cohesion must be float64")
         if state.dim() != 2 or state.shape[0] != N_PTS_ARRAYS or cohesion.shape != (state.shape[1],):
             raise ValueError("state must be (28, n) and cohesion (n,)")
         n = state.shape[1]
-        h = MPMHandle(_params_with_E(prms, youngs_modulus.item()), n, PRECISION_FP64_SVD64, device)
+        h = MPMHandle(_params_with_E(prms, youngs_modulus.item()), n, precision, device)
         try:
             h.upload(state.detach().cpu().numpy(), cohesion=cohesion.detach().cpu().numpy())
             hist = h.adjoint_forward(int(nsteps), int(ckpt_every))
@@ -79,12 +83,13 @@ class IndenterForceHistory(torch.autograd.Function):
             ctx.handle = None
         dev = ctx.out_device
         return (g_state, torch.from_numpy(dc).to(dev), torch.tensor(dE, dtype=torch.float64, device=dev),
-                None, None, None, None)
+                None, None, None, None, None)
 
 
-def indenter_force_history(state, cohesion, youngs_modulus, prms, nsteps, ckpt_every=20, device=0):
+def indenter_force_history(state, cohesion, youngs_modulus, prms, nsteps, ckpt_every=20, device=0,
+                           precision=PRECISION_FP64_SVD64):
     """(nsteps, 3) indenter force of each substep, differentiable with respect
     to state, cohesion and youngs_modulus (see the module docstring)."""
     if not torch.is_tensor(youngs_modulus):
         youngs_modulus = torch.tensor(float(youngs_modulus), dtype=torch.float64)
-    return IndenterForceHistory.apply(state, cohesion, youngs_modulus, prms, nsteps, ckpt_every, device)
+    return IndenterForceHistory.apply(state, cohesion, youngs_modulus, prms, nsteps, ckpt_every, device, precision)

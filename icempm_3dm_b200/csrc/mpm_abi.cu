@@ -117,6 +117,8 @@ struct mpm_handle {
     double* adj_gb7 = nullptr;        // grid adjoints: vb, mb, Pb (7 x gstride)
     int adj_steps = 0, adj_every = 0;
     bool adj_ready = false;
+    double* adj_force = nullptr;      // force history of a mixed adjoint forward (3 per substep)
+    int adj_force_cap = 0;
 
     int p2g_variant = 5;              // see mpm_testing_set_p2g_variant (5: pair-merged, 6 per SM)
     int g2p_variant = 0;              // see mpm_testing_set_g2p_variant (0: 4 blocks of 128 per SM)
@@ -228,6 +230,7 @@ void free_all(mpm_handle* h) {
     h->ckpt.clear();
     h->seg.clear();
     cudaFree(h->adj_A); cudaFree(h->adj_cgrad); cudaFree(h->adj_Egrad); cudaFree(h->adj_g7); cudaFree(h->adj_gb7);
+    cudaFree(h->adj_force);
     for (int* p : h->scan_levels) cudaFree(p);
     h->scan_levels.clear();
     cudaFree(h->fr_f); cudaFree(h->fr_status); cudaFree(h->fr_last); cudaFree(h->fr_i); cudaFree(h->fr_rec);
@@ -1409,12 +1412,67 @@ AdjParams adj_params(const mpm_handle* h) {
 
 }  // namespace
 
+namespace {
+
+// While the adjoint recomputes and reverses, a mixed handle is driven as an
+// FP64 one with the FP64 SVD, on its FP64 staging rows and FP64 grid.
+struct Fp64View {
+    mpm_handle* h;
+    int saved;
+    explicit Fp64View(mpm_handle* hh) : h(hh), saved(hh->precision) {
+        if (is_mixed(h)) h->precision = MPM_PRECISION_FP64_SVD64;
+    }
+    ~Fp64View() { h->precision = saved; }
+};
+
+// Mixed forward of the adjoint: the mixed step in segments of ckpt_every
+// substeps (each segment's last substep stores v and C), the FP64 staging
+// of the state at every segment start as its checkpoint, the force history
+// collected in h->adj_force. No sort runs meanwhile (the reverse sweep keeps
+// per-particle adjoints by slot).
+int adjoint_forward_mixed(mpm_handle* h, int nsteps, int every) {
+    const int saved_interval = h->sort_interval;
+    h->sort_interval = 0;
+    int r = MPM_OK;
+    for (int s0 = 0; s0 < nsteps && !r; s0 += every) {
+        if ((r = mixed_to_staging(h))) break;
+        CK(h, cudaMemcpyAsync(h->ckpt[s0 / every], h->pts, state_bytes(h), cudaMemcpyDeviceToDevice, h->stream));
+        h->ckpt_prms[s0 / every] = h->prms;
+        const int m = std::min(every, nsteps - s0);
+        if ((r = mpm_step(h, m, nullptr))) break;
+        CK(h, cudaMemcpyAsync(h->adj_force + 3 * (size_t)s0, h->force_steps, sizeof(double) * 3 * (size_t)m,
+                              cudaMemcpyDeviceToDevice, h->stream));
+    }
+    h->sort_interval = saved_interval;
+    return r;
+}
+
+}  // namespace
+
 extern "C" int mpm_adjoint_forward(mpm_handle* h, int nsteps, int ckpt_every, double* force_hist) {
     if (!h || nsteps <= 0 || ckpt_every <= 0) return MPM_ERR_ARG;
     if (!h->uploaded) return MPM_ERR_STATE;
-    if (is_mixed(h)) return MPM_ERR_ARG;   // the adjoint differentiates the FP64 step
     int r = ensure_adjoint_buffers(h, nsteps, ckpt_every);
     if (r) return r;
+    if (is_mixed(h)) {
+        if (nsteps > h->adj_force_cap) {
+            CK(h, cudaStreamSynchronize(h->stream));
+            cudaFree(h->adj_force);
+            h->adj_force = nullptr;
+            CK(h, cudaMalloc(&h->adj_force, sizeof(double) * 3 * (size_t)nsteps));
+            h->adj_force_cap = nsteps;
+        }
+        h->adj_ready = false;
+        if ((r = adjoint_forward_mixed(h, nsteps, ckpt_every))) return r;
+        if (force_hist)
+            CK(h, cudaMemcpyAsync(force_hist, h->adj_force, sizeof(double) * 3 * (size_t)nsteps,
+                                  cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        h->adj_steps = nsteps;
+        h->adj_every = ckpt_every;
+        h->adj_ready = true;
+        return MPM_OK;
+    }
     if (nsteps > h->force_steps_cap) {
         CK(h, cudaStreamSynchronize(h->stream));
         cudaFree(h->force_steps);
@@ -1444,6 +1502,7 @@ extern "C" int mpm_adjoint_forward(mpm_handle* h, int nsteps, int ckpt_every, do
 extern "C" int mpm_adjoint_backward(mpm_handle* h, const double* dL_dforce, double* dL_dcohesion, double* dL_dE) {
     if (!h || !dL_dforce) return MPM_ERR_ARG;
     if (!h->adj_ready) return MPM_ERR_STATE;
+    const Fp64View fp64(h);
     const int N = h->adj_steps, k = h->adj_every, n = (int)h->n;
     const DevParams dp = h->dp;
     const AdjParams q = adj_params(h);

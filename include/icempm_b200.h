@@ -207,11 +207,13 @@ int  mpm_count(mpm_handle* h, unsigned* n);
  * No counterpart in the reference (new, for calibrating ice strength).
  * Reverse-mode gradients of a loss on the indenter force history with
  * respect to per-particle cohesion and Young's modulus, through the FP64 step
- * (FP64 precision modes; MPM_ERR_ARG on a mixed handle). */
+ * (FP64 SVD). On a mixed handle the forward runs in mixed precision and the
+ * reverse sweep recomputes each segment in FP64 from its checkpoint. */
 
 /* Runs nsteps substeps exactly as mpm_step (no sorting) from the current
- * state, saving the particle state every ckpt_every substeps on the device;
- * force_hist (may be NULL) receives nsteps x 3 forces. The state advances. */
+ * state, saving the particle state every ckpt_every substeps on the device
+ * (on a mixed handle: the FP64 copy of the mixed state); force_hist (may be
+ * NULL) receives nsteps x 3 forces. The state advances. */
 int  mpm_adjoint_forward(mpm_handle* h, int nsteps, int ckpt_every, double* force_hist);
 /* Reverse sweep of the last mpm_adjoint_forward: each segment is recomputed
  * from its checkpoint, then reversed substep by substep. dL_dforce: nsteps x 3

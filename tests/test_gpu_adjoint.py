@@ -169,3 +169,40 @@ def test_single_call_adjoint_equals_forward_then_backward():
     # two GPU runs differ only by the summation order of FP64 atomics
     assert np.allclose(dc, dc2, rtol=1e-8, atol=1e-8 * np.abs(dc2).max())
     assert dE.value == pytest.approx(dE2, rel=1e-8)
+
+
+def test_mixed_forward_adjoint_follows_the_fp64_adjoint():
+    """The calibration row's mixed forward: mpm_adjoint_forward on a mixed
+    handle runs the mixed step (checkpoints = FP64 copies of the mixed state)
+    and the backward recomputes each segment in FP64. Its force history is
+    the mixed step's, and its gradients follow the FP64-forward adjoint's to
+    the distance between the two trajectories."""
+    from icempm_3dm_b200 import PRECISION_MIXED
+    prms, soa, coh = case(n=3000, seed=11)
+    n = soa.shape[1]
+    nsteps, every = 40, 10
+    rng = np.random.default_rng(3)
+    wgt = rng.standard_normal((nsteps, 3))
+    wgt[:, 2] = 0.0
+    out = {}
+    for prec in (PRECISION_FP64_SVD64, PRECISION_MIXED):
+        with MPMHandle(prms, n, prec) as h:
+            h.upload(soa, cohesion=coh)
+            hist = np.zeros((nsteps, 3))
+            check(LIB.mpm_adjoint_forward(h._h, nsteps, every, dptr(hist)), "adjoint forward")
+            dc = np.zeros(n)
+            dE = ctypes.c_double(0)
+            check(LIB.mpm_adjoint_backward(h._h, dptr(np.ascontiguousarray(wgt)), dptr(dc), ctypes.byref(dE)),
+                  "adjoint backward")
+            out[prec] = (hist, dc, dE.value)
+        with MPMHandle(prms, n, prec) as h:
+            h.upload(soa, cohesion=coh)
+            ref = h.step(nsteps)
+        assert np.linalg.norm(out[prec][0] - ref) <= 1e-6 * np.linalg.norm(ref), prec
+    (h64, dc64, dE64), (hmx, dcmx, dEmx) = out[PRECISION_FP64_SVD64], out[PRECISION_MIXED]
+    e_hist = np.linalg.norm(hmx - h64) / np.linalg.norm(h64)
+    e_c = np.abs(dcmx - dc64).max() / np.abs(dc64).max()
+    e_E = abs(dEmx - dE64) / abs(dE64)
+    print(f"\nmixed vs FP64 forward: force history {e_hist:.2e}; dL/dc {e_c:.2e} of the largest; dL/dE {e_E:.2e}")
+    assert np.count_nonzero(dcmx) > n // 2
+    assert e_hist < 1e-3 and e_c < 1e-2 and e_E < 1e-2

@@ -54,7 +54,12 @@ def test_autograd_matches_c_abi_and_dual_forward_mode():
     assert torch.count_nonzero(state.grad[4:10]) > 0
 
 
-def test_calibration_recovers_strength_scales():
+@pytest.mark.parametrize("forward", ["fp64", "mixed"])
+def test_calibration_recovers_strength_scales(forward):
+    """The target history comes from the FP64 forward (c x 1.2, E x 0.9);
+    the fit runs its forward in FP64 or, as the calibration workload asks,
+    in mixed precision (gradients from the FP64 recompute of each segment)."""
+    from icempm_3dm_b200 import PRECISION_MIXED
     """Force history measured with cohesion x1.2 and E x0.9 (the calibration
     workload's targets) on a 20k-particle copy of that block; the fit starts at
     x1. Crush flags switch inside the fit, so the loss is piecewise smooth and
@@ -74,8 +79,9 @@ def test_calibration_recovers_strength_scales():
         crushed = float(np.mean((h.download()[IDX_UTILITY].view(np.int64) & 0x10000) != 0))
     assert crushed > 0.02            # cohesion must matter
     sc, sE, losses = calibrate_strength(soa, coh, prms.YoungsModulus, prms, measured, nsteps, ckpt_every=20,
-                                        iters=40)
-    print(f"\ncrushed {crushed:.3f}; cohesion scale {sc:.5f}  E scale {sE:.5f}  "
+                                        iters=40,
+                                        precision=PRECISION_MIXED if forward == "mixed" else PRECISION_FP64_SVD64)
+    print(f"\n{forward} forward: crushed {crushed:.3f}; cohesion scale {sc:.5f}  E scale {sE:.5f}  "
           f"loss {losses[0]:.3e} -> {losses[-1]:.3e} in {len(losses)} evaluations")
     assert losses[-1] < 1e-2 * losses[0]
     assert abs(sc - 1.2) < 1e-2 and abs(sE - 0.9) < 1e-2
