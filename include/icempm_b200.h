@@ -85,8 +85,9 @@ int  mpm_params_parse_string(SimParams3D* prms, const char* json_text,
 /* GPU_Implementation6::initialize + allocate_arrays + update_constants
  * (gpu_implementation6.cpp:380-398, 446-462, 583-586;
  *  gpu_partition_3d.cu:218-309). One partition on `device`.
- * `capacity` = number of particles the handle can hold. The grid is
- * GridXTotal x GridY x GridZ nodes (no halo slabs: one partition).
+ * `capacity` = number of particles the handle can hold. The grid is the
+ * reference's one-partition buffer, (GridXTotal + 2 GridHaloSize) x GridY x
+ * GridZ nodes (GridHaloSize = 0 needs no halo slabs with one partition).
  * *status receives 0 or an error code; NULL is returned on error. */
 mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity,
                        int device, int* status);
