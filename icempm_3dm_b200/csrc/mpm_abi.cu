@@ -119,6 +119,7 @@ struct mpm_handle {
     bool adj_ready = false;
     double* adj_force = nullptr;      // force history of a mixed adjoint forward (3 per substep)
     int adj_force_cap = 0;
+    std::vector<double*> adj_gcache;  // P2G grid of each substep of the segment being reversed
 
     int p2g_variant = 5;              // see mpm_testing_set_p2g_variant (5: pair-merged, 6 per SM)
     int g2p_variant = 0;              // see mpm_testing_set_g2p_variant (0: 4 blocks of 128 per SM)
@@ -231,6 +232,8 @@ void free_all(mpm_handle* h) {
     h->seg.clear();
     cudaFree(h->adj_A); cudaFree(h->adj_cgrad); cudaFree(h->adj_Egrad); cudaFree(h->adj_g7); cudaFree(h->adj_gb7);
     cudaFree(h->adj_force);
+    for (double* c : h->adj_gcache) cudaFree(c);
+    h->adj_gcache.clear();
     for (int* p : h->scan_levels) cudaFree(p);
     h->scan_levels.clear();
     cudaFree(h->fr_f); cudaFree(h->fr_status); cudaFree(h->fr_last); cudaFree(h->fr_i); cudaFree(h->fr_rec);
@@ -1358,14 +1361,18 @@ namespace {
 
 size_t state_bytes(const mpm_handle* h) { return sizeof(double) * MPM_N_PTS_ARRAYS * h->pitch; }
 
-// One FP64 substep of Model3D::Step on the particle rows at h->pts.
-int fp64_substep(mpm_handle* h, double* force3) {
+// One FP64 substep of Model3D::Step on the particle rows at h->pts;
+// p2g_copy (may be null) receives the grid after P2G (4 x gstride doubles).
+int fp64_substep(mpm_handle* h, double* force3, double* p2g_copy = nullptr) {
     SimParams3D& p = h->prms;
     p.SimulationTime += p.InitialTimeStep;
     p.indenter_x = p.indenter_x_initial + p.SimulationTime * p.IndVelocity;
     int r;
     if ((r = reset_grid(h))) return r;
     if ((r = launch_p2g(h))) return r;
+    if (p2g_copy)
+        CK(h, cudaMemcpyAsync(p2g_copy, h->grid, sizeof(double) * 4 * (size_t)h->dp.gstride, cudaMemcpyDeviceToDevice,
+                              h->stream));
     if ((r = launch_update(h, p.indenter_x, p.indenter_y, force3))) return r;
     const int record = (p.SimulationStep % p.UpdateEveryNthStep) == 0;
     if ((r = launch_g2p(h, record))) return r;
@@ -1384,6 +1391,11 @@ int ensure_adjoint_buffers(mpm_handle* h, int nsteps, int every) {
         double* b = nullptr;
         CK(h, cudaMalloc(&b, state_bytes(h)));
         h->seg.push_back(b);
+    }
+    while ((int)h->adj_gcache.size() < every) {
+        double* b = nullptr;
+        CK(h, cudaMalloc(&b, sizeof(double) * 4 * (size_t)h->dp.gstride));
+        h->adj_gcache.push_back(b);
     }
     h->ckpt_prms.resize(nck);
     if (!h->adj_A) {
@@ -1524,7 +1536,7 @@ extern "C" int mpm_adjoint_backward(mpm_handle* h, const double* dL_dforce, doub
             double* next = h->seg[s - s0 + 1];
             CK(h, cudaMemcpyAsync(next, h->seg[s - s0], state_bytes(h), cudaMemcpyDeviceToDevice, h->stream));
             h->pts = next;
-            r = fp64_substep(h, h->force_phase);
+            r = fp64_substep(h, h->force_phase, h->adj_gcache[s - s0]);
             sp[s - s0] = h->prms;   // holds this substep's indenter position
         }
         h->pts = pts_final;
@@ -1534,8 +1546,9 @@ extern "C" int mpm_adjoint_backward(mpm_handle* h, const double* dL_dforce, doub
             const double* Sn = h->seg[s - s0];
             const double* Sn1 = h->seg[s - s0 + 1];
             const double ix = sp[s - s0].indenter_x, iy = sp[s - s0].indenter_y;
-            CK(h, cudaMemsetAsync(h->adj_g7, 0, sizeof(double) * 4 * gs, h->stream));
-            k_p2g_pairs_f64<6><<<blocks_for(n, 128), 128, 0, h->stream>>>(dp, Sn, h->pitch, n, h->adj_g7, h->err);
+            // the substep's P2G grid, as the recompute produced it
+            CK(h, cudaMemcpyAsync(h->adj_g7, h->adj_gcache[s - s0], sizeof(double) * 4 * gs, cudaMemcpyDeviceToDevice,
+                                  h->stream));
             k_adj_update_record<256><<<blocks_for(dp.nodes, 256), 256, 0, h->stream>>>(dp, h->adj_g7, ix, iy);
             CK(h, cudaMemsetAsync(h->adj_gb7, 0, sizeof(double) * 7 * gs, h->stream));
             k_adj_g2p_rev<128><<<blocks_for(n, 128), 128, 0, h->stream>>>(dp, q, Sn, Sn1, h->pitch, n, h->adj_g7, h->p0,
