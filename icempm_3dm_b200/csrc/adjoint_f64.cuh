@@ -357,6 +357,9 @@ __global__ void __launch_bounds__(BLOCK) k_adj_g2p_rev(DevParams P, AdjParams Q,
             fx[d] = x[d] * P.h_inv - (double)base[d];
         }
         quad_w_dw(fx, w, dw);
+        double dwh[3][3];   // weight derivatives per unit length (d/dx = d/dfx / h)
+        for (int k = 0; k < 3; k++)
+            for (int d = 0; d < 3; d++) dwh[k][d] = dw[k][d] * P.h_inv;
         // recompute v', C'
         double vp[3] = {0, 0, 0}, Cp[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         for (int a = 0; a < 3; a++)
@@ -424,8 +427,8 @@ __global__ void __launch_bounds__(BLOCK) k_adj_g2p_rev(DevParams P, AdjParams Q,
                     if (!node_inside(P, nx, ny, nz)) continue;
                     const long long ni = node_index(P, nx, ny, nz);
                     const double wt = w[a][0] * w[b][1] * w[c][2];
-                    const double gw[3] = {dw[a][0] * w[b][1] * w[c][2] / h, w[a][0] * dw[b][1] * w[c][2] / h,
-                                          w[a][0] * w[b][1] * dw[c][2] / h};
+                    const double gw[3] = {dwh[a][0] * w[b][1] * w[c][2], w[a][0] * dwh[b][1] * w[c][2],
+                                          w[a][0] * w[b][1] * dwh[c][2]};
                     const double nv[3] = {g7[4 * P.gstride + ni], g7[5 * P.gstride + ni], g7[6 * P.gstride + ni]};
                     const double dd[3] = {(a - fx[0]) * h, (b - fx[1]) * h, (c - fx[2]) * h};
                     double gsc = 0;
@@ -578,6 +581,9 @@ __global__ void __launch_bounds__(BLOCK) k_adj_p2g_rev(DevParams P, AdjParams Q,
             fx[d] = x[d] * P.h_inv - (double)base[d];
         }
         quad_w_dw(fx, w, dw);
+        double dwh[3][3];   // weight derivatives per unit length (d/dx = d/dfx / h)
+        for (int k = 0; k < 3; k++)
+            for (int d = 0; d < 3; d++) dwh[k][d] = dw[k][d] * P.h_inv;
         double xb[3] = {0, 0, 0}, sP[3] = {0, 0, 0}, Qb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         for (int a = 0; a < 3; a++)
             for (int b = 0; b < 3; b++)
@@ -586,8 +592,8 @@ __global__ void __launch_bounds__(BLOCK) k_adj_p2g_rev(DevParams P, AdjParams Q,
                     if (!node_inside(P, nx, ny, nz)) continue;
                     const long long ni = node_index(P, nx, ny, nz);
                     const double wt = w[a][0] * w[b][1] * w[c][2];
-                    const double gw[3] = {dw[a][0] * w[b][1] * w[c][2] / h, w[a][0] * dw[b][1] * w[c][2] / h,
-                                          w[a][0] * w[b][1] * dw[c][2] / h};
+                    const double gw[3] = {dwh[a][0] * w[b][1] * w[c][2], w[a][0] * dwh[b][1] * w[c][2],
+                                          w[a][0] * w[b][1] * dwh[c][2]};
                     const double mb = gadj[3 * P.gstride + ni];
                     const double Pb[3] = {gadj[4 * P.gstride + ni], gadj[5 * P.gstride + ni], gadj[6 * P.gstride + ni]};
                     const double dd[3] = {(a - fx[0]) * h, (b - fx[1]) * h, (c - fx[2]) * h};

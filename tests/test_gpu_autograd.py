@@ -78,8 +78,10 @@ def test_calibration_recovers_strength_scales(forward):
         measured = h.step(nsteps)
         crushed = float(np.mean((h.download()[IDX_UTILITY].view(np.int64) & 0x10000) != 0))
     assert crushed > 0.02            # cohesion must matter
+    # L-BFGS runs to convergence here (its evaluation cap is 1.25 x iters): with 40
+    # iterations it could stop at the cap, 1 % away along the shallow c/E trade-off
     sc, sE, losses = calibrate_strength(soa, coh, prms.YoungsModulus, prms, measured, nsteps, ckpt_every=20,
-                                        iters=40,
+                                        iters=100,
                                         precision=PRECISION_MIXED if forward == "mixed" else PRECISION_FP64_SVD64)
     print(f"\n{forward} forward: crushed {crushed:.3f}; cohesion scale {sc:.5f}  E scale {sE:.5f}  "
           f"loss {losses[0]:.3e} -> {losses[-1]:.3e} in {len(losses)} evaluations")
