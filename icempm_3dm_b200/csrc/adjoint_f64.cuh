@@ -360,22 +360,10 @@ __global__ void __launch_bounds__(BLOCK) k_adj_g2p_rev(DevParams P, AdjParams Q,
         double dwh[3][3];   // weight derivatives per unit length (d/dx = d/dfx / h)
         for (int k = 0; k < 3; k++)
             for (int d = 0; d < 3; d++) dwh[k][d] = dw[k][d] * P.h_inv;
-        // recompute v', C'
-        double vp[3] = {0, 0, 0}, Cp[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-        for (int a = 0; a < 3; a++)
-            for (int b = 0; b < 3; b++)
-                for (int c = 0; c < 3; c++) {
-                    const int nx = base[0] + a, ny = base[1] + b, nz = base[2] + c;
-                    if (!node_inside(P, nx, ny, nz)) continue;
-                    const long long ni = node_index(P, nx, ny, nz);
-                    const double wt = w[a][0] * w[b][1] * w[c][2];
-                    const double nv[3] = {g7[4 * P.gstride + ni], g7[5 * P.gstride + ni], g7[6 * P.gstride + ni]};
-                    const double dd[3] = {(a - fx[0]) * h, (b - fx[1]) * h, (c - fx[2]) * h};
-                    for (int r = 0; r < 3; r++) {
-                        vp[r] += wt * nv[r];
-                        for (int k = 0; k < 3; k++) Cp[r][k] += s4 * wt * nv[r] * dd[k];
-                    }
-                }
+        // C' of this substep: the G2P that produced S1 stored it (the Bp rows)
+        double Cp[3][3];
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) Cp[r][c] = S1[(MPM_BP00 + 3 * r + c) * pitch + i];
         double Am[3][3], Ftr[3][3];
         for (int r = 0; r < 3; r++)
             for (int c = 0; c < 3; c++) Am[r][c] = (r == c ? 1.0 : 0.0) + dt * Cp[r][c];
