@@ -45,3 +45,52 @@ def test_create_without_device_fails_cleanly():
     st = ctypes.c_int(-1)
     h = LIB.mpm_create(p, 0, 100, 0, ctypes.byref(st))
     assert not h and st.value == 103
+
+
+C_PROGRAM = r"""
+#include <stdio.h>
+#include <string.h>
+#include "icempm_b200.h"
+#include "icempm_b200_testing.h"
+
+int main(void) {
+    SimParams3D p;
+    char raw[256];
+    int st = -1;
+    mpm_params_reset(&p);
+    if (mpm_params_parse_string(&p, "{\"InputRawPoints\": \"pc.h5\", \"GridX\": 64, \"GridY\": 27, "
+                                    "\"GridZ\": 56, \"DomainDimensionX\": 3.3}", raw, (int)sizeof raw) != 0)
+        return 2;
+    if (strcmp(raw, "pc.h5") != 0 || p.GridXTotal != 64 || p.GridZ != 56) return 3;
+    if (mpm_testing_sizeof_params() != sizeof(SimParams3D)) return 4;
+    if (sizeof(mpm_visual_point) != 32 || sizeof(mpm_update_pos) != 28 || sizeof(mpm_update_jp) != 8 ||
+        sizeof(mpm_update_status) != 8)
+        return 5;
+    mpm_handle* h = mpm_create(&p, MPM_PRECISION_MIXED, 1000, 0, &st);
+    if (h) { mpm_destroy(h); printf("device\n"); return 0; }
+    printf("status %d\n", st);
+    return st == MPM_ERR_NO_DEVICE ? 0 : 6;
+}
+"""
+
+
+def test_headers_compile_as_c_and_a_c_program_links_and_runs(tmp_path):
+    """include/*.h are plain C99: a C program includes both headers, links
+    against libicempm_b200.so and calls it (parameters, struct layouts,
+    mpm_create, which without a GPU reports MPM_ERR_NO_DEVICE)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        return
+    src = tmp_path / "abi.c"
+    src.write_text(C_PROGRAM)
+    exe = tmp_path / "abi"
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                        str(src), "-L", libdir, "-licempm_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert r.stdout.strip() in ("device", "status 103")
