@@ -19,7 +19,7 @@ import math
 
 import numpy as np
 
-from ._lib import (BP00, FE00, IDX_JP_INV, LIB, N_PTS_ARRAYS, POSX, SimParams3D)
+from ._lib import (FE00, IDX_JP_INV, LIB, N_PTS_ARRAYS, POSX, SimParams3D)
 
 _M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
 

@@ -4,7 +4,7 @@ branches of the step."""
 import numpy as np
 
 from icempm_3dm_b200 import generator as gen
-from icempm_3dm_b200._lib import (BP00, FE00, IDX_JP_INV, IDX_UTILITY, STATUS_CRUSHED, STATUS_DISABLED,
+from icempm_3dm_b200._lib import (BP00, FE00, IDX_JP_INV, IDX_UTILITY, STATUS_CRUSHED,
                                   STATUS_LIQUID, VELX)
 
 

@@ -17,7 +17,7 @@ import pytest
 
 from icempm_3dm_b200 import MPMHandle, PRECISION_FP64, PRECISION_FP64_SVD64, PRECISION_MIXED
 from icempm_3dm_b200 import generator as gen
-from icempm_3dm_b200._lib import BP00, FE00, IDX_JP_INV, IDX_UTILITY, LIB, POSX, STATUS_CRUSHED, VELX
+from icempm_3dm_b200._lib import BP00, FE00, IDX_JP_INV, IDX_UTILITY, POSX, STATUS_CRUSHED, VELX
 from oracle import pyoracle as po
 
 pytestmark = pytest.mark.gpu

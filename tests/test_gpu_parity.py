@@ -10,8 +10,8 @@ import pytest
 
 from icempm_3dm_b200 import MPMHandle, PRECISION_FP64, PRECISION_FP64_SVD64, PRECISION_MIXED
 from icempm_3dm_b200 import generator as gen
-from icempm_3dm_b200._lib import (BP00, FE00, IDX_JP_INV, IDX_P, IDX_Q, IDX_UTILITY, LIB, POSX, STATUS_DISABLED,
-                                  VELX, check, dptr)
+from icempm_3dm_b200._lib import (BP00, IDX_JP_INV, IDX_P, IDX_Q, IDX_UTILITY, LIB, POSX, STATUS_DISABLED, check,
+                                  dptr)
 from oracle import pyoracle as po
 from tests.helpers import close, perturbed_block, util_as_double, util_bits
 

@@ -7,8 +7,8 @@ import numpy as np
 import pytest
 
 from icempm_3dm_b200 import generator as gen
-from icempm_3dm_b200._lib import (BP00, FE00, IDX_JP_INV, IDX_P, IDX_Q, IDX_UTILITY, LIB, POSX, STATUS_CRUSHED,
-                                  STATUS_DISABLED, VELX)
+from icempm_3dm_b200._lib import (BP00, FE00, IDX_P, IDX_Q, IDX_UTILITY, LIB, POSX, STATUS_CRUSHED, STATUS_DISABLED,
+                                  VELX)
 from oracle import pyoracle as po
 from tests.helpers import perturbed_block, util_as_double, util_bits
 
