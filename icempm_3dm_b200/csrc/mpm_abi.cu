@@ -621,6 +621,16 @@ mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity
             st = MPM_ERR_ARG;
             break;
         }
+        if ((long long)(prms->GridXTotal + 2 * prms->GridHaloSize) * prms->GridY * prms->GridZ >= 0x7fffffffLL) {
+            st = MPM_ERR_ARG;   // node indices are 32-bit in the kernels
+            break;
+        }
+        if (precision == MPM_PRECISION_MIXED &&
+            std::max(prms->GridXTotal + 2 * prms->GridHaloSize, std::max(prms->GridY, prms->GridZ)) >=
+                (1 << (31 - kFixBits)) - 1) {
+            st = MPM_ERR_ARG;   // positions are x / h in 32-bit fixed point with kFixBits fraction bits
+            break;
+        }
         int count = 0;
         if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0 || device < 0 || device >= count) {
             cudaGetLastError();
@@ -630,10 +640,6 @@ mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity
         cudaDeviceProp prop;
         if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) {
             st = MPM_ERR_NO_DEVICE;
-            break;
-        }
-        if ((long long)(prms->GridXTotal + 2 * prms->GridHaloSize) * prms->GridY * prms->GridZ >= 0x7fffffffLL) {
-            st = MPM_ERR_ARG;   // node indices are 32-bit in the kernels
             break;
         }
         h = new (std::nothrow) mpm_handle();

@@ -87,7 +87,10 @@ int  mpm_params_parse_string(SimParams3D* prms, const char* json_text,
  *  gpu_partition_3d.cu:218-309). One partition on `device`.
  * `capacity` = number of particles the handle can hold. The grid is the
  * reference's one-partition buffer, (GridXTotal + 2 GridHaloSize) x GridY x
- * GridZ nodes (GridHaloSize = 0 needs no halo slabs with one partition).
+ * GridZ nodes (GridHaloSize = 0 needs no halo slabs with one partition),
+ * fewer than 2^31 of them. MPM_PRECISION_MIXED holds positions as x / h in
+ * 32-bit fixed point with 20 fraction bits: each grid dimension (x with its
+ * halo slabs) must be below 2047 cells. Otherwise MPM_ERR_ARG.
  * *status receives 0 or an error code; NULL is returned on error. */
 mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity,
                        int device, int* status);

@@ -94,3 +94,20 @@ def test_headers_compile_as_c_and_a_c_program_links_and_runs(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
     assert r.stdout.strip() in ("device", "status 103")
+
+
+def test_create_rejects_grids_the_kernels_cannot_index():
+    """Argument checks come before the device probe: more than 2^31 nodes,
+    or (mixed precision) a grid dimension of 2047 cells or more, which the
+    32-bit fixed-point positions (20 fraction bits) cannot reach."""
+    p = SimParams3D()
+    LIB.mpm_params_reset(p)
+    st = ctypes.c_int(-1)
+    p.GridXTotal, p.GridY, p.GridZ = 2100, 50, 50
+    assert not LIB.mpm_create(p, 1, 100, 0, ctypes.byref(st)) and st.value == 101
+    h = LIB.mpm_create(p, 0, 100, 0, ctypes.byref(st))      # FP64 takes that grid
+    if h:
+        LIB.mpm_destroy(h)
+    assert st.value != 101
+    p.GridXTotal, p.GridY, p.GridZ = 1500, 1500, 1000
+    assert not LIB.mpm_create(p, 0, 100, 0, ctypes.byref(st)) and st.value == 101
