@@ -330,15 +330,48 @@ struct AdjParams {
     double s4;   // 4 / h^2
 };
 
+// Vector-Jacobian product of the return map (mpm_kernels.cuh:494-544) for
+// the points crushed in this substep, ahead of k_adj_g2p_rev: rmv rows 0-8
+// receive dL/dF_tr, row 9 dL/dJp_inv; the cohesion and E terms go to cgrad
+// and Egrad. Kept apart from k_adj_g2p_rev so that the dual-number sweep's
+// registers do not set that kernel's occupancy.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_adj_rm_vjp(DevParams P, AdjParams Q, const double* __restrict__ S0,
+                                                      const double* __restrict__ S1, size_t pitch, int n,
+                                                      const double* __restrict__ p0arr, const double* __restrict__ A,
+                                                      double* __restrict__ rmv, double* __restrict__ cgrad,
+                                                      double* __restrict__ Egrad) {
+    const int i = blockIdx.x * BLOCK + threadIdx.x;
+    double eg = 0;
+    const long long util = i < n ? __double_as_longlong(S0[i]) : kDisabled;
+    if (!(util & kDisabled) && !(util & kLiquid) && (__double_as_longlong(S1[i]) & kCrushed)) {
+        const double dt = P.dt;
+        double F[3][3], Am[3][3], Ftr9[9], Fb1[9], g[13];
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) {
+                F[r][c] = S0[(MPM_FE00 + 3 * r + c) * pitch + i];
+                Am[r][c] = (r == c ? 1.0 : 0.0) + dt * S1[(MPM_BP00 + 3 * r + c) * pitch + i];
+            }
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) Ftr9[3 * r + c] = Am[r][0] * F[0][c] + Am[r][1] * F[1][c] + Am[r][2] * F[2][c];
+        for (int k = 0; k < 9; k++) Fb1[k] = A[(ADJ_F + k) * pitch + i];
+        const double Jpb1 = A[ADJ_JP * pitch + i];
+        const double p0 = p0arr ? p0arr[i] : P.p0;
+        rm_vjp(Q.rc, Ftr9, S0[MPM_IDX_JP_INV * pitch + i], p0, P.mu, P.kappa, Fb1, Jpb1, g);
+        for (int k = 0; k < 10; k++) rmv[k * pitch + i] = g[k];
+        cgrad[i] += g[10] / Q.rc.tan_phi;
+        eg = g[11] * Q.dmu_dE + g[12] * Q.dkappa_dE;
+    }
+    block_add_double(eg, Egrad);
+}
+
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_adj_g2p_rev(DevParams P, AdjParams Q, const double* __restrict__ S0,
                                                        const double* __restrict__ S1, size_t pitch, int n,
                                                        const double* __restrict__ g7,
-                                                       const double* __restrict__ p0arr, double* __restrict__ A,
-                                                       double* __restrict__ gadj, double* __restrict__ cgrad,
-                                                       double* __restrict__ Egrad) {
+                                                       const double* __restrict__ rmv, double* __restrict__ A,
+                                                       double* __restrict__ gadj) {
     const int i = blockIdx.x * BLOCK + threadIdx.x;
-    double eg = 0;
     const long long util = i < n ? __double_as_longlong(S0[i]) : kDisabled;
     if (!(util & kDisabled)) {
         const long long util1 = __double_as_longlong(S1[i]);
@@ -346,70 +379,91 @@ __global__ void __launch_bounds__(BLOCK) k_adj_g2p_rev(DevParams P, AdjParams Q,
         const bool crushed = !liquid && (util1 & kCrushed);
         const double h = P.h, dt = P.dt, s4 = Q.s4;
         double x[3], F[3][3];
+#pragma unroll
         for (int d = 0; d < 3; d++) x[d] = S0[(MPM_POSX + d) * pitch + i];
+#pragma unroll
         for (int r = 0; r < 3; r++)
+#pragma unroll
             for (int c = 0; c < 3; c++) F[r][c] = S0[(MPM_FE00 + 3 * r + c) * pitch + i];
         const double Jp = S0[MPM_IDX_JP_INV * pitch + i];
         int base[3];
         double fx[3], w[3][3], dw[3][3];
+#pragma unroll
         for (int d = 0; d < 3; d++) {
             base[d] = (int)(x[d] * P.h_inv - 0.5);
             fx[d] = x[d] * P.h_inv - (double)base[d];
         }
         quad_w_dw(fx, w, dw);
         double dwh[3][3];   // weight derivatives per unit length (d/dx = d/dfx / h)
+#pragma unroll
         for (int k = 0; k < 3; k++)
+#pragma unroll
             for (int d = 0; d < 3; d++) dwh[k][d] = dw[k][d] * P.h_inv;
         // C' of this substep: the G2P that produced S1 stored it (the Bp rows)
         double Cp[3][3];
+#pragma unroll
         for (int r = 0; r < 3; r++)
+#pragma unroll
             for (int c = 0; c < 3; c++) Cp[r][c] = S1[(MPM_BP00 + 3 * r + c) * pitch + i];
         double Am[3][3], Ftr[3][3];
+#pragma unroll
         for (int r = 0; r < 3; r++)
+#pragma unroll
             for (int c = 0; c < 3; c++) Am[r][c] = (r == c ? 1.0 : 0.0) + dt * Cp[r][c];
+#pragma unroll
         for (int r = 0; r < 3; r++)
+#pragma unroll
             for (int c = 0; c < 3; c++) Ftr[r][c] = Am[r][0] * F[0][c] + Am[r][1] * F[1][c] + Am[r][2] * F[2][c];
         // adjoints of S_{n+1}
         double xb[3], vb[3], Cb[3][3], Fb1[9], Jpb1;
+#pragma unroll
         for (int d = 0; d < 3; d++) { xb[d] = A[(ADJ_X + d) * pitch + i]; vb[d] = A[(ADJ_V + d) * pitch + i]; }
+#pragma unroll
         for (int k = 0; k < 9; k++) { Cb[k / 3][k % 3] = A[(ADJ_C + k) * pitch + i]; Fb1[k] = A[(ADJ_F + k) * pitch + i]; }
         Jpb1 = A[ADJ_JP * pitch + i];
         // return map (and liquid volume update)
         double Ftrb[3][3], Jpb0 = Jpb1, Ab[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
         for (int k = 0; k < 9; k++) Ftrb[k / 3][k % 3] = Fb1[k];
         if (crushed) {
-            const double p0 = p0arr ? p0arr[i] : P.p0;
-            double Ftr9[9], g[13];
-            for (int k = 0; k < 9; k++) Ftr9[k] = Ftr[k / 3][k % 3];
-            rm_vjp(Q.rc, Ftr9, Jp, p0, P.mu, P.kappa, Fb1, Jpb1, g);
-            for (int k = 0; k < 9; k++) Ftrb[k / 3][k % 3] = g[k];
-            Jpb0 = g[9];
-            cgrad[i] += g[10] / Q.rc.tan_phi;
-            eg += g[11] * Q.dmu_dE + g[12] * Q.dkappa_dE;
+            // the return map's VJP, from k_adj_rm_vjp (which also took its
+            // cohesion and E terms)
+#pragma unroll
+            for (int k = 0; k < 9; k++) Ftrb[k / 3][k % 3] = rmv[k * pitch + i];
+            Jpb0 = rmv[9 * pitch + i];
         } else if (liquid) {
             const double detA = det3(Am);
             double cof[3][3];
             cofactor(Am, cof);
             Jpb0 = Jpb1 * detA;
+#pragma unroll
             for (int r = 0; r < 3; r++)
+#pragma unroll
                 for (int c = 0; c < 3; c++) Ab[r][c] += Jpb1 * Jp * cof[r][c];
         }
         // F_tr = A F
         double Fb0[3][3];
+#pragma unroll
         for (int r = 0; r < 3; r++)
+#pragma unroll
             for (int c = 0; c < 3; c++) {
                 Ab[r][c] += Ftrb[r][0] * F[c][0] + Ftrb[r][1] * F[c][1] + Ftrb[r][2] * F[c][2];
                 Fb0[r][c] = Am[0][r] * Ftrb[0][c] + Am[1][r] * Ftrb[1][c] + Am[2][r] * Ftrb[2][c];
             }
         double Cbt[3][3], vbt[3];
+#pragma unroll
         for (int r = 0; r < 3; r++) {
             vbt[r] = vb[r] + dt * xb[r];
+#pragma unroll
             for (int c = 0; c < 3; c++) Cbt[r][c] = Cb[r][c] + dt * Ab[r][c];
         }
         // gather adjoint: node velocity adjoints and x-gradients
         double xb0[3] = {xb[0], xb[1], xb[2]};
+#pragma unroll
         for (int a = 0; a < 3; a++)
+#pragma unroll
             for (int b = 0; b < 3; b++)
+#pragma unroll
                 for (int c = 0; c < 3; c++) {
                     const int nx = base[0] + a, ny = base[1] + b, nz = base[2] + c;
                     if (!node_inside(P, nx, ny, nz)) continue;
@@ -420,27 +474,30 @@ __global__ void __launch_bounds__(BLOCK) k_adj_g2p_rev(DevParams P, AdjParams Q,
                     const double nv[3] = {g7[4 * P.gstride + ni], g7[5 * P.gstride + ni], g7[6 * P.gstride + ni]};
                     const double dd[3] = {(a - fx[0]) * h, (b - fx[1]) * h, (c - fx[2]) * h};
                     double gsc = 0;
+#pragma unroll
                     for (int r = 0; r < 3; r++) {
                         const double cd = Cbt[r][0] * dd[0] + Cbt[r][1] * dd[1] + Cbt[r][2] * dd[2];
                         atomicAdd(gadj + r * P.gstride + ni, wt * vbt[r] + s4 * wt * cd);
                         gsc += nv[r] * (vbt[r] + s4 * cd);
                     }
+#pragma unroll
                     for (int d = 0; d < 3; d++) {
                         const double ctv = Cbt[0][d] * nv[0] + Cbt[1][d] * nv[1] + Cbt[2][d] * nv[2];
                         xb0[d] += gw[d] * gsc - s4 * wt * ctv;
                     }
                 }
+#pragma unroll
         for (int d = 0; d < 3; d++) {
             A[(ADJ_X + d) * pitch + i] = xb0[d];
             A[(ADJ_V + d) * pitch + i] = 0.0;
         }
+#pragma unroll
         for (int k = 0; k < 9; k++) {
             A[(ADJ_C + k) * pitch + i] = 0.0;
             A[(ADJ_F + k) * pitch + i] = Fb0[k / 3][k % 3];
         }
         A[ADJ_JP * pitch + i] = Jpb0;
     }
-    block_add_double(eg, Egrad);
 }
 
 // ---------------------------------------------------------- reverse node
@@ -541,11 +598,14 @@ __global__ void __launch_bounds__(BLOCK) k_adj_p2g_rev(DevParams P, AdjParams Q,
         const double h = P.h;
         const double mass = liquid ? P.liquid_mass : P.particle_mass;
         double x[3], v[3], C[3][3], F[3][3];
+#pragma unroll
         for (int d = 0; d < 3; d++) {
             x[d] = S0[(MPM_POSX + d) * pitch + i];
             v[d] = S0[(MPM_VELX + d) * pitch + i];
         }
+#pragma unroll
         for (int r = 0; r < 3; r++)
+#pragma unroll
             for (int c = 0; c < 3; c++) {
                 C[r][c] = S0[(MPM_BP00 + 3 * r + c) * pitch + i];
                 F[r][c] = S0[(MPM_FE00 + 3 * r + c) * pitch + i];
@@ -554,27 +614,37 @@ __global__ void __launch_bounds__(BLOCK) k_adj_p2g_rev(DevParams P, AdjParams Q,
         double tau[3][3];
         if (liquid) {
             const double pw = water_pressure(P, Jp);
+#pragma unroll
             for (int r = 0; r < 3; r++)
+#pragma unroll
                 for (int c = 0; c < 3; c++) tau[r][c] = r == c ? pw : 0.0;
         } else {
             kirchhoff_wolper(P, F, tau);
         }
         double Qm[3][3];
+#pragma unroll
         for (int r = 0; r < 3; r++)
+#pragma unroll
             for (int c = 0; c < 3; c++) Qm[r][c] = mass * C[r][c] - P.dt_vol_Dpinv * tau[r][c];
         int base[3];
         double fx[3], w[3][3], dw[3][3];
+#pragma unroll
         for (int d = 0; d < 3; d++) {
             base[d] = (int)(x[d] * P.h_inv - 0.5);
             fx[d] = x[d] * P.h_inv - (double)base[d];
         }
         quad_w_dw(fx, w, dw);
         double dwh[3][3];   // weight derivatives per unit length (d/dx = d/dfx / h)
+#pragma unroll
         for (int k = 0; k < 3; k++)
+#pragma unroll
             for (int d = 0; d < 3; d++) dwh[k][d] = dw[k][d] * P.h_inv;
         double xb[3] = {0, 0, 0}, sP[3] = {0, 0, 0}, Qb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
         for (int a = 0; a < 3; a++)
+#pragma unroll
             for (int b = 0; b < 3; b++)
+#pragma unroll
                 for (int c = 0; c < 3; c++) {
                     const int nx = base[0] + a, ny = base[1] + b, nz = base[2] + c;
                     if (!node_inside(P, nx, ny, nz)) continue;
@@ -586,12 +656,15 @@ __global__ void __launch_bounds__(BLOCK) k_adj_p2g_rev(DevParams P, AdjParams Q,
                     const double Pb[3] = {gadj[4 * P.gstride + ni], gadj[5 * P.gstride + ni], gadj[6 * P.gstride + ni]};
                     const double dd[3] = {(a - fx[0]) * h, (b - fx[1]) * h, (c - fx[2]) * h};
                     double g = mass * mb;
+#pragma unroll
                     for (int r = 0; r < 3; r++) {
                         const double cr = mass * v[r] + Qm[r][0] * dd[0] + Qm[r][1] * dd[1] + Qm[r][2] * dd[2];
                         g += Pb[r] * cr;
                         sP[r] += wt * Pb[r];
+#pragma unroll
                         for (int k = 0; k < 3; k++) Qb[r][k] += wt * Pb[r] * dd[k];
                     }
+#pragma unroll
                     for (int d = 0; d < 3; d++) {
                         const double qtp = Qm[0][d] * Pb[0] + Qm[1][d] * Pb[1] + Qm[2][d] * Pb[2];
                         xb[d] += gw[d] * g - wt * qtp;
@@ -599,7 +672,9 @@ __global__ void __launch_bounds__(BLOCK) k_adj_p2g_rev(DevParams P, AdjParams Q,
                 }
         // Q = m C - k tau
         double Fb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, tb[3][3];
+#pragma unroll
         for (int r = 0; r < 3; r++)
+#pragma unroll
             for (int c = 0; c < 3; c++) tb[r][c] = -P.dt_vol_Dpinv * Qb[r][c];
         double mub = 0, kb = 0, Jpb = 0;
         if (liquid) {
@@ -610,10 +685,12 @@ __global__ void __launch_bounds__(BLOCK) k_adj_p2g_rev(DevParams P, AdjParams Q,
             kirchhoff_vjp(P.mu, P.kappa, F, tb, Fb, mub, kb);
         }
         eg += mub * Q.dmu_dE + kb * Q.dkappa_dE;
+#pragma unroll
         for (int d = 0; d < 3; d++) {
             A[(ADJ_X + d) * pitch + i] += xb[d];
             A[(ADJ_V + d) * pitch + i] = mass * sP[d];
         }
+#pragma unroll
         for (int k = 0; k < 9; k++) {
             A[(ADJ_C + k) * pitch + i] = mass * Qb[k / 3][k % 3];
             A[(ADJ_F + k) * pitch + i] += Fb[k / 3][k % 3];

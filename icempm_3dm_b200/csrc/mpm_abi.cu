@@ -120,6 +120,7 @@ struct mpm_handle {
     double* adj_force = nullptr;      // force history of a mixed adjoint forward (3 per substep)
     int adj_force_cap = 0;
     std::vector<double*> adj_gcache;  // P2G grid of each substep of the segment being reversed
+    double* adj_rmv = nullptr;        // return-map VJP of the crushed points (10 x pitch)
 
     int p2g_variant = 5;              // see mpm_testing_set_p2g_variant (5: pair-merged, 6 per SM)
     int g2p_variant = 0;              // see mpm_testing_set_g2p_variant (0: 4 blocks of 128 per SM)
@@ -234,6 +235,7 @@ void free_all(mpm_handle* h) {
     cudaFree(h->adj_force);
     for (double* c : h->adj_gcache) cudaFree(c);
     h->adj_gcache.clear();
+    cudaFree(h->adj_rmv);
     for (int* p : h->scan_levels) cudaFree(p);
     h->scan_levels.clear();
     cudaFree(h->fr_f); cudaFree(h->fr_status); cudaFree(h->fr_last); cudaFree(h->fr_i); cudaFree(h->fr_rec);
@@ -1410,6 +1412,7 @@ int ensure_adjoint_buffers(mpm_handle* h, int nsteps, int every) {
         CK(h, cudaMalloc(&h->adj_Egrad, sizeof(double)));
         CK(h, cudaMalloc(&h->adj_g7, sizeof(double) * 7 * (size_t)h->dp.gstride));
         CK(h, cudaMalloc(&h->adj_gb7, sizeof(double) * 7 * (size_t)h->dp.gstride));
+        CK(h, cudaMalloc(&h->adj_rmv, sizeof(double) * 10 * h->pitch));
     }
     return MPM_OK;
 }
@@ -1557,9 +1560,10 @@ extern "C" int mpm_adjoint_backward(mpm_handle* h, const double* dL_dforce, doub
                                   h->stream));
             k_adj_update_record<256><<<blocks_for(dp.nodes, 256), 256, 0, h->stream>>>(dp, h->adj_g7, ix, iy);
             CK(h, cudaMemsetAsync(h->adj_gb7, 0, sizeof(double) * 7 * gs, h->stream));
-            k_adj_g2p_rev<128><<<blocks_for(n, 128), 128, 0, h->stream>>>(dp, q, Sn, Sn1, h->pitch, n, h->adj_g7, h->p0,
-                                                                         h->adj_A, h->adj_gb7, h->adj_cgrad,
-                                                                         h->adj_Egrad);
+            k_adj_rm_vjp<128><<<blocks_for(n, 128), 128, 0, h->stream>>>(dp, q, Sn, Sn1, h->pitch, n, h->p0, h->adj_A,
+                                                                        h->adj_rmv, h->adj_cgrad, h->adj_Egrad);
+            k_adj_g2p_rev<128><<<blocks_for(n, 128), 128, 0, h->stream>>>(dp, q, Sn, Sn1, h->pitch, n, h->adj_g7,
+                                                                         h->adj_rmv, h->adj_A, h->adj_gb7);
             k_adj_node_rev<256><<<blocks_for(dp.nodes, 256), 256, 0, h->stream>>>(
                 dp, h->adj_g7, h->adj_gb7, ix, iy, dL_dforce[3 * s], dL_dforce[3 * s + 1], dL_dforce[3 * s + 2]);
             k_adj_p2g_rev<128><<<blocks_for(n, 128), 128, 0, h->stream>>>(dp, q, Sn, h->pitch, n, h->adj_gb7, h->adj_A,
