@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(BLOCK) k_adj_rm_vjp(DevParams P, AdjParams Q, 
 }
 
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_adj_g2p_rev(DevParams P, AdjParams Q, const double* __restrict__ S0,
+__global__ void __launch_bounds__(BLOCK, 3) k_adj_g2p_rev(DevParams P, AdjParams Q, const double* __restrict__ S0,
                                                        const double* __restrict__ S1, size_t pitch, int n,
                                                        const double* __restrict__ g7,
                                                        const double* __restrict__ rmv, double* __restrict__ A,
@@ -587,7 +587,7 @@ __global__ void __launch_bounds__(BLOCK) k_adj_node_rev(DevParams P, const doubl
 // ----------------------------------------------------------- reverse P2G
 
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_adj_p2g_rev(DevParams P, AdjParams Q, const double* __restrict__ S0,
+__global__ void __launch_bounds__(BLOCK, 4) k_adj_p2g_rev(DevParams P, AdjParams Q, const double* __restrict__ S0,
                                                        size_t pitch, int n, const double* __restrict__ gadj,
                                                        double* __restrict__ A, double* __restrict__ Egrad) {
     const int i = blockIdx.x * BLOCK + threadIdx.x;
