@@ -83,3 +83,20 @@ def test_partial_warps_and_blocks_match_oracle(n, precision):
         else:
             assert np.abs(hist).max() < 1e-6
         assert np.abs(out[POSX:POSX + 3] - sim.soa[POSX:POSX + 3]).max() < 1e-6
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_frame_records_of_empty_and_fully_disabled_inputs(precision):
+    """mpm_frame_records with no particles, or with every particle disabled:
+    the scans run over a single sentinel element and no record comes out."""
+    prms, soa = perturbed_block(n=300, seed=6)
+    with MPMHandle(prms, 300, precision) as h:
+        h.upload(np.ascontiguousarray(soa[:, :0]))
+        assert h.frame_records(0, True).size == 0
+        assert all(r.size == 0 for r in h.frame_records(1, False))
+        bits = util_bits(soa) | STATUS_DISABLED
+        soa[IDX_UTILITY] = util_as_double(bits)
+        h.upload(soa)
+        assert h.frame_records(2, True).size == 0
+        h.step(2)
+        assert all(r.size == 0 for r in h.frame_records(3, False))
