@@ -746,6 +746,7 @@ int mpm_upload_soa(mpm_handle* h, const double* soa, unsigned pitch, unsigned n)
     h->n = n;
     h->uploaded = true;
     h->p2g_ready = false;
+    h->fr_ready = false;   // new points: the next frame record must be a full frame
     if (is_mixed(h)) {
         int r = mixed_from_staging(h);
         if (r) return r;

@@ -151,8 +151,8 @@ typedef struct { int32_t idx; uint8_t status, pad[3]; } mpm_update_status;      
  * full != 0 (SaveFrame without a previous frame): keeps every particle as
  * the visual state, with `frame` as its last position refresh, and copies
  * the VisualPoint records to `points` (*n_points of them; room for the
- * particle count). full == 0 (needs a full frame first, else
- * MPM_ERR_STATE): for each particle, in order,
+ * particle count). full == 0 (needs a full frame since the last
+ * mpm_upload_soa, else MPM_ERR_STATE): for each particle, in order,
  *   |pos - (vpos + vvel * (float)(dt * (frame - last) * UpdateEveryNthStep))|
  *   > animation_threshold_pos -> an UpdatePos record, last = frame;
  *   |vJp_inv - Jp_inv| > 1e-2  -> an UpdateJp record;

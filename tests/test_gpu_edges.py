@@ -97,6 +97,8 @@ def test_frame_records_of_empty_and_fully_disabled_inputs(precision):
         bits = util_bits(soa) | STATUS_DISABLED
         soa[IDX_UTILITY] = util_as_double(bits)
         h.upload(soa)
+        with pytest.raises(Exception):
+            h.frame_records(2, False)           # an upload asks for a full frame first
         assert h.frame_records(2, True).size == 0
         h.step(2)
         assert all(r.size == 0 for r in h.frame_records(3, False))
