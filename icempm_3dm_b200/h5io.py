@@ -128,11 +128,21 @@ class H5File:
         end = bytes(self._b[data + off:data + size]).index(b"\0")
         return bytes(self._b[data + off:data + off + end]).decode()
 
+    def _check(self, a, n):
+        if a < 0 or a + n > len(self._b):
+            raise H5Error(f"structure at {a} runs past the end of the file")
+
     def _read_group(self, btree, heap):
         data, size = self._heap(heap)
-        stack = [btree]
+        self._check(data, size)
+        stack, seen = [btree], set()
         while stack:
-            a = self._a(stack.pop())
+            addr = stack.pop()
+            if addr in seen:
+                raise H5Error("group B-tree revisits a node")
+            seen.add(addr)
+            a = self._a(addr)
+            self._check(a, 24)
             if bytes(self._b[a:a + 4]) != b"TREE" or self._b[a + 4] != 0:
                 raise H5Error("group B-tree node expected")
             level, used = self._b[a + 5], self._u(a + 6, 2)
@@ -147,9 +157,12 @@ class H5File:
 
     def _read_snod(self, addr, data, size):
         a = self._a(addr)
+        self._check(a, 8)
         if bytes(self._b[a:a + 4]) != b"SNOD":
             raise H5Error("symbol table node signature missing")
-        for k in range(self._u(a + 6, 2)):
+        nsym = self._u(a + 6, 2)
+        self._check(a + 8, 40 * nsym)
+        for k in range(nsym):
             e = a + 8 + 40 * k
             name = self._heap_name(data, size, self._u(e, 8))
             self._datasets[name] = self._u(e + 8, 8)
@@ -157,17 +170,25 @@ class H5File:
     # -- object headers
     def _messages(self, addr):
         a = self._a(addr)
+        self._check(a, 16)
         if bytes(self._b[a:a + 4]) == b"OHDR":
             raise H5Error("version 2 object headers are not read")
         if self._b[a] != 1:
             raise H5Error(f"object header version {self._b[a]}")
         blocks = [(a + 16, self._u(a + 8, 4))]
+        seen = set()
         out = []
         while blocks:
             p, n = blocks.pop(0)
+            if p in seen:
+                raise H5Error("object header continuation revisits a block")
+            seen.add(p)
+            self._check(p, n)
             end = p + n
             while p + 8 <= end:
                 t, sz, fl = self._u(p, 2), self._u(p + 2, 2), self._b[p + 4]
+                if p + 8 + sz > end:
+                    raise H5Error("header message runs past its block")
                 d = bytes(self._b[p + 8:p + 8 + sz])
                 if t == 0x10:
                     blocks.append((self._a(int.from_bytes(d[0:8], "little")), int.from_bytes(d[8:16], "little")))
@@ -213,7 +234,9 @@ class H5File:
     def read(self, name):
         info = self._info(name)
         shape, dt, lay = info["shape"], info["dtype"], info["layout"]
-        count = int(np.prod(shape)) if shape else 1
+        count = int(np.prod(shape, dtype=object)) if shape else 1
+        if count * dt.itemsize > 1 << 40:
+            raise H5Error(f"{name}: dataspace {shape} of {dt} is beyond 1 TiB")
         if lay[0] == "compact":
             return np.frombuffer(lay[1], dtype=dt, count=count).reshape(shape).copy()
         if lay[0] == "contiguous":
@@ -223,6 +246,7 @@ class H5File:
             if size < count * dt.itemsize:
                 raise H5Error(f"{name}: contiguous storage smaller than the dataspace")
             a = self._a(addr)
+            self._check(a, count * dt.itemsize)
             return np.frombuffer(self._b[a:a + count * dt.itemsize], dtype=dt).reshape(shape).copy()
         return self._read_chunked(name, shape, dt, lay[1], lay[2], info["filters"])
 
@@ -235,6 +259,9 @@ class H5File:
         cbytes = int(np.prod(cshape)) * dt.itemsize
         for off, size, mask, addr in self._chunks(btree, rank):
             a = self._a(addr)
+            self._check(a, size)
+            if any(o >= s for o, s in zip(off, shape)):
+                raise H5Error(f"{name}: chunk offset {off} outside the dataspace {shape}")
             raw = bytes(self._b[a:a + size])
             raw = _unfilter(raw, filters, mask, dt.itemsize)
             if len(raw) != cbytes:
@@ -247,12 +274,18 @@ class H5File:
 
     def _chunks(self, btree, rank):
         ks = 8 + 8 * (rank + 1)
-        stack = [btree]
+        stack, seen = [btree], set()
         while stack:
-            a = self._a(stack.pop())
+            addr = stack.pop()
+            if addr in seen:
+                raise H5Error("chunk B-tree revisits a node")
+            seen.add(addr)
+            a = self._a(addr)
+            self._check(a, 24)
             if bytes(self._b[a:a + 4]) != b"TREE" or self._b[a + 4] != 1:
                 raise H5Error("chunk B-tree node expected")
             level, used = self._b[a + 5], self._u(a + 6, 2)
+            self._check(a + 24, used * (ks + 8) + ks)
             p = a + 24
             for i in range(used):
                 size, mask = self._u(p, 4), self._u(p + 4, 4)
@@ -412,7 +445,10 @@ def _unfilter(raw, filters, mask, elem):
             continue
         fid = filters[i][0]
         if fid == FILTER_DEFLATE:
-            raw = zlib.decompress(raw)       # zlib stream; Adler-32 checked
+            try:
+                raw = zlib.decompress(raw)   # zlib stream; Adler-32 checked
+            except zlib.error as e:
+                raise H5Error(f"deflate stream: {e}") from None
         elif fid == FILTER_SHUFFLE:
             es = filters[i][2][0] if filters[i][2] else elem
             n = len(raw) // es
@@ -512,6 +548,8 @@ class H5Writer:
     def create_dataset(self, name, data, chunks=None, deflate=None, attrs=None):
         if any(s[0] == name for s in self._sets):
             raise H5Error(f"dataset {name} exists")
+        if not name or "/" in name or "\0" in name:
+            raise H5Error(f"dataset name {name!r}: datasets are written under the root group only")
         data = np.asarray(data)
         if data.ndim == 0:
             data = data.reshape(1)

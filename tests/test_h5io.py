@@ -135,3 +135,34 @@ def test_reader_rejects_what_it_does_not_read(tmp_path):
     with pytest.raises(h5io.H5Error):
         with h5io.H5Writer(tmp_path / "c.h5") as w:
             w.create_dataset("s", np.array(["a"]))
+
+
+@needs_ref
+def test_damaged_copies_of_the_reference_file_raise_and_do_not_hang(tmp_path):
+    """Truncations and byte corruptions of a real file end in an exception
+    (H5Error, or an index/value error from numpy on garbage), never in a hang."""
+    data = bytearray(open(REF_H5, "rb").read())
+    rng = np.random.default_rng(0)
+    cases = [data[:n] for n in (100, 700, 1100, 5000, 300000, len(data) // 2)]
+    for _ in range(40):
+        d = bytearray(data)
+        for pos in rng.integers(0, 3000, 4):        # metadata region: superblock, heap, B-trees, headers
+            d[pos] = rng.integers(0, 256)
+        cases.append(d)
+    for k, d in enumerate(cases):
+        p = tmp_path / f"d{k}.h5"
+        p.write_bytes(bytes(d))
+        try:
+            with h5io.H5File(p) as f:
+                for name in f.keys():
+                    f.read(name)
+                    f.attrs(name)
+        except (h5io.H5Error, KeyError, ValueError, IndexError, UnicodeDecodeError, OverflowError, TypeError,
+                MemoryError):
+            pass
+
+
+def test_writer_rejects_names_outside_the_root_group(tmp_path):
+    with pytest.raises(h5io.H5Error):
+        with h5io.H5Writer(tmp_path / "n.h5") as w:
+            w.create_dataset("a/b", np.zeros(3))
