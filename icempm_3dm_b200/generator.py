@@ -306,4 +306,4 @@ def calibration_block(n=20_000, penetration_cells=3, ind_velocity=2.0, cohesion_
 
 __all__ = ["BlockConfig", "CONFIGS", "make_block", "make_grains_block", "make_params", "small_block",
            "calibration_block",
-           "jittered_lattice", "splitmix64", "uniform", "normal", "BP00"]
+           "jittered_lattice", "splitmix64", "uniform", "normal"]

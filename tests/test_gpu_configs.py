@@ -5,8 +5,11 @@
   block8m    mixed vs FP64 (FP64 SVD) on the GPU, 2,000 substeps: force
              history within 1e-3 relative (the required bound) and the error
              of each output field, printed.
-  calib      the calibration block (20,000-particle copy): adjoint vs central
-             differences (eps 1e-4 relative) on 64 random particles' cohesion.
+  calib      the calibration workload: adjoint vs central differences (eps
+             1e-4 relative) on 64 random particles' cohesion, on the 20,000-
+             particle copy and on the full 500,000-particle block (plus its 8
+             largest gradients and E); adjoint vs the FP64 dual-number forward
+             mode on the 20,000-particle copy over 200 substeps.
   grains30m  the non-uniform 30 M case: mixed vs FP64 force history, and
              size-independent properties (sorted cell keys, finite state).
 """
@@ -17,7 +20,7 @@ import pytest
 
 from icempm_3dm_b200 import MPMHandle, PRECISION_FP64, PRECISION_FP64_SVD64, PRECISION_MIXED
 from icempm_3dm_b200 import generator as gen
-from icempm_3dm_b200._lib import BP00, FE00, IDX_JP_INV, IDX_UTILITY, POSX, STATUS_CRUSHED, VELX
+from icempm_3dm_b200._lib import BP00, FE00, IDX_JP_INV, IDX_UTILITY, LIB, POSX, STATUS_CRUSHED, VELX
 from oracle import pyoracle as po
 
 pytestmark = pytest.mark.gpu
@@ -149,6 +152,94 @@ def test_calibration_block_adjoint_vs_central_differences_on_64_particles():
           f"({err.max() / scale:.2e} of the largest gradient), non-zero there: {int(np.count_nonzero(ad))}")
     assert scale > 0
     assert err.max() <= 1e-3 * scale
+
+
+def test_calib500k_adjoint_vs_central_differences_at_full_size():
+    """The calibration workload at its own size (500,000 particles, 200
+    substeps, checkpoints every 20, FP64 forward): adjoint vs central
+    differences (eps 1e-4 relative) on 64 random particles' cohesion, on the
+    8 particles with the largest gradients (few of 500,000 crush near the
+    indenter, so random ones mostly have none) and on E."""
+    prms, soa, coh = gen.calibration_block(n=500_000)
+    n = soa.shape[1]
+    steps, every = 200, 20
+    rng = np.random.default_rng(6)
+    wgt = rng.standard_normal((steps, 3))
+    wgt[:, 2] = 0.0
+    h = MPMHandle(prms, n, PRECISION_FP64_SVD64)
+
+    def loss(c, p=None):
+        if p is not None:
+            h.update_constants(p)
+        h.upload(soa, cohesion=c)
+        out = float(np.sum(wgt * h.step(steps)))
+        if p is not None:
+            h.update_constants(prms)
+        return out
+
+    try:
+        h.upload(soa, cohesion=coh)
+        h.adjoint_forward(steps, every)
+        dc, dE = h.adjoint_backward(wgt)
+        pick = np.concatenate([rng.choice(n, 64, replace=False), np.argsort(-np.abs(dc))[:8]])
+        eps = 1e-4
+        fd = np.empty(pick.size)
+        for k, i in enumerate(pick):
+            cp, cm = coh.copy(), coh.copy()
+            cp[i] *= 1 + eps
+            cm[i] *= 1 - eps
+            fd[k] = (loss(cp) - loss(cm)) / (2 * eps * coh[i])
+        E0 = prms.YoungsModulus
+
+        def with_E(E):
+            p = prms.copy()
+            p.YoungsModulus = E
+            LIB.mpm_params_compute_camclay(p)
+            LIB.mpm_params_compute_helper_variables(p)
+            return p
+
+        fdE = (loss(coh, with_E(E0 * (1 + eps))) - loss(coh, with_E(E0 * (1 - eps)))) / (2 * eps * E0)
+    finally:
+        h.close()
+    ad = dc[pick]
+    scale = float(np.abs(dc).max())
+    err = np.abs(fd - ad)
+    top = slice(64, None)
+    print(f"\ncalib500k: {int(np.count_nonzero(dc))} of {n} cohesion gradients non-zero; 64 random: max |fd - adj| "
+          f"{err[:64].max():.2e} ({int(np.count_nonzero(ad[:64]))} non-zero); 8 largest: max rel "
+          f"{(err[top] / np.abs(ad[top])).max():.2e}; E: fd {fdE:.6e} adjoint {dE:.6e}")
+    assert scale > 0
+    assert err[:64].max() <= 1e-3 * scale
+    assert np.all(err[top] <= 1e-3 * np.abs(ad[top]))
+    assert abs(fdE - dE) <= 1e-3 * abs(dE)
+
+
+def test_calibration_copy_adjoint_vs_dual_numbers_over_200_substeps():
+    """The calibration workload's second check: on the 20,000-particle copy,
+    200 substeps with checkpoints every 20, the adjoint against the oracle's
+    FP64 dual-number forward mode along E and along a random cohesion
+    direction (both exact derivatives: they differ by rounding and the
+    order of the FP64 atomics)."""
+    prms, soa, coh = gen.calibration_block()
+    n = soa.shape[1]
+    steps, every = 200, 20
+    rng = np.random.default_rng(8)
+    wgt = rng.standard_normal((steps, 3))
+    wgt[:, 2] = 0.0
+    with MPMHandle(prms, n, PRECISION_FP64_SVD64) as h:
+        h.upload(soa, cohesion=coh)
+        h.adjoint_forward(steps, every)
+        dc, dE = h.adjoint_backward(wgt)
+    p0 = coh / prms.DP_tan_phi
+    _, dhist_E, _, _ = po.dual_steps(prms, soa, steps, p0=p0, dE=1.0)
+    r = coh * rng.standard_normal(n)
+    _, dhist_c, _, _ = po.dual_steps(prms, soa, steps, p0=p0, dp0=r / prms.DP_tan_phi)
+    tE, tc = float(np.sum(wgt * dhist_E)), float(np.sum(wgt * dhist_c))
+    print(f"\ncalibration copy, 200 substeps: E dual {tE:.12e} adjoint {dE:.12e}; cohesion direction dual "
+          f"{tc:.12e} adjoint {float(r @ dc):.12e}")
+    assert tE != 0 and tc != 0
+    assert abs(tE - dE) <= 1e-6 * abs(tE)
+    assert abs(tc - float(r @ dc)) <= 1e-6 * abs(tc)
 
 
 @pytest.fixture(scope="module")
