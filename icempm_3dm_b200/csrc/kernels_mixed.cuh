@@ -1196,10 +1196,11 @@ __device__ __forceinline__ void fused_payload(const DevParams& P, bool active, c
 // SCATTER: 0 = warp-reduced direct float4 atomics, 1 = direct float4
 // atomics, 2 = FP32 shared-memory tile, 3 = int32 fixed-point shared-memory
 // tile (2 and 3 fall back to 0 when the box is too big), 4 = direct float4
-// atomics with same-cell pairs merged. GATHER: 0 = from the grid through
-// L1, 1 = from the warp's velocity box staged in shared memory by the warp's
-// loads (dynamic shared memory of 4 x kVBoxNodes float4), 2 = the box brought
-// in by one TMA tensor copy per warp (4 x kTmaSliceNodes float4; vel_map).
+// atomics with same-cell pairs merged, 5 = split scatter of merged pairs.
+// GATHER: 0 = from the grid through L1, 1 = from the warp's velocity box
+// staged in shared memory by the warp's loads (dynamic shared memory of
+// 4 x kVBoxNodes float4), 2 = the box brought in by one TMA tensor copy per
+// warp (4 x kTmaSliceNodes float4; vel_map).
 constexpr int kVBoxNodes = 256;
 template <int MINB, int SCATTER, int GATHER = 0>
 __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedState s, int n,

@@ -404,7 +404,7 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
     if (h->mixed_gather == 2 && h->vel_map_ok) {
         // TMA gather box: 4 warps x kTmaSliceNodes float4 of dynamic shared memory
         const size_t tmsm = sizeof(float4) * 4 * kTmaSliceNodes;
-        if (sc == 4)
+        if (sc >= 4)   // the pair-merged scatters (9, 10) run as 9 here
             k_g2p2g_mixed<8, 4, 2><<<nb, 128, tmsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,
                                                                  record_pq, store_vc, h->err, 0, h->rm_list, rm_count,
                                                                  h->vel_map);
@@ -423,7 +423,7 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
                                                             record_pq, store_vc, h->err, 0, h->rm_list, rm_count,  \
                                                             h->vel_map)
         if (h->mixed_variant == 1) {
-            if (sc == 4) FUSED_G(5, 4);
+            if (sc >= 4) FUSED_G(5, 4);
             else if (sc == 0) FUSED_G(5, 0);
             else FUSED_G(5, 1);
         } else if (h->mixed_variant == 3) {
@@ -431,7 +431,7 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
             else if (sc == 4) FUSED_G(8, 4);
             else FUSED_G(8, 1);
         } else {
-            if (sc == 4) FUSED_G(6, 4);
+            if (sc >= 4) FUSED_G(6, 4);
             else if (sc == 0) FUSED_G(6, 0);
             else FUSED_G(6, 1);
         }
@@ -445,7 +445,7 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
                                                          record_pq, store_vc, h->err, kMixedTileNodes, h->rm_list,  \
                                                          rm_count, h->vel_map)
 #define FUSED_SC(MINB)                  \
-    if (sc == 4) FUSED(MINB, 4);        \
+    if (sc >= 4) FUSED(MINB, 4);        \
     else if (sc == 3) FUSED(MINB, 3);   \
     else if (sc == 2) FUSED(MINB, 2);   \
     else if (sc == 1) FUSED(MINB, 1);   \

@@ -24,8 +24,8 @@ extern "C" {
  * 8 = int32 block fixed-point shared-memory tile, 9 = float4 atomics with
  * same-cell particle pairs merged in registers (default), 10 = split
  * scatter: a same-cell pair exchanges its payloads once and each lane adds
- * both particles' contributions over half of the stencil (with G2P
- * variant 5, the default; with the other gathers 10 runs as 9). */
+ * both particles' contributions over half of the stencil. 10 needs G2P
+ * variant 5 (the default); with the other gathers it runs as 9. */
 int mpm_testing_set_p2g_variant(mpm_handle* h, int variant);
 
 /* G2P kernel occupancy target (FP64 modes): 0 = 4 blocks of 128 threads per
