@@ -2,6 +2,8 @@
 
   block250k  FP64 GPU vs the CPU oracle (reference semantics, FP32 SVD),
              1,000 substeps: indenter force per substep and final state.
+  block2m    FP64 at scale with lognormal per-particle cohesion, GPU vs the
+             oracle over 400 substeps.
   block8m    mixed vs FP64 (FP64 SVD) on the GPU, 2,000 substeps: force
              history within 1e-3 relative (the required bound) and the error
              of each output field, printed.
@@ -88,6 +90,53 @@ def test_block250k_fp64_matches_oracle_over_1000_substeps():
             assert e_ref <= max(5 * e_run, 1e-3)
             assert x_ref <= max(5 * x_run, 1e-6)
     print("\nblock250k FP64 vs oracle: " + "; ".join(lines))
+
+
+def test_block2m_fp64_with_lognormal_cohesion_matches_oracle():
+    """The FP64-at-scale workload (2,000,000 particles, h 0.0125 m, lognormal
+    per-particle cohesion, indenter at 0.5 m/s) on the GPU against the oracle
+    on the host cores, with the same apex shift p0 = c / tan(phi) per particle
+    (the device forms it with the same correctly rounded division). 400
+    substeps: the span in which rounding differences of the FP64 atomics'
+    order have not yet met a discrete switch (block250k above)."""
+    prms, soa, coh = gen.make_block(gen.CONFIGS["block2m"])
+    n = soa.shape[1]
+    perm = po.sort_permutation(prms, soa, n)
+    soa = np.ascontiguousarray(soa[:, perm])
+    coh = np.ascontiguousarray(coh[perm])
+    assert coh.std() > 0.2 * coh.mean()   # non-uniform strength
+    p0 = coh / prms.DP_tan_phi
+    marks = (200, 400)
+    hist, outs = [], []
+    with MPMHandle(prms, n, PRECISION_FP64) as h:
+        h.upload(soa, cohesion=coh)
+        done = 0
+        for m in marks:
+            hist.append(h.step(m - done))
+            done = m
+            outs.append(h.download())
+    hist = np.concatenate(hist)
+    sim = po.OracleSim(prms, soa, n, p0=p0, svd_mode=0, nthreads=os.cpu_count() or 1)
+    ref_hist, ref_out, done = [], [], 0
+    for m in marks:
+        hh, err = sim.step(m - done)
+        assert err == 0
+        done = m
+        ref_hist.append(hh)
+        ref_out.append(sim.soa.copy())
+    ref_hist = np.concatenate(ref_hist)
+    assert np.linalg.norm(ref_hist[:, 0]) > 0
+    lines = []
+    for k, m in enumerate(marks):
+        e = rel(hist[:m], ref_hist[:m])
+        x = float(np.abs(outs[k][POSX:POSX + 3] - ref_out[k][POSX:POSX + 3]).max())
+        f = rel(outs[k][FE00:FE00 + 9], ref_out[k][FE00:FE00 + 9])
+        flips = int(np.sum(crushed(outs[k]) != crushed(ref_out[k])))
+        lines.append(f"{m} substeps: force {e:.2e}, positions {x:.2e} m, F {f:.2e}, "
+                     f"crushed {int(crushed(outs[k]).sum())}, flag differences {flips}")
+        assert e < 1e-7 and x < 1e-10 and f < 1e-9
+        assert flips <= n * 1e-5
+    print("\nblock2m FP64 vs oracle: " + "; ".join(lines))
 
 
 def test_block8m_mixed_force_history_within_1e3_of_fp64_over_2000_substeps():
