@@ -16,7 +16,9 @@ with the force history read back, SoA downloaded) inside the timed region. N > 1
 replicas, one per GPU (the path is one partition; no collective).
 
 --impl reference times the CPU port of the reference step (the oracle,
-OpenMP on all host cores) on the same workload.
+OpenMP on all host cores): exactly K substeps, each over a bounded sample of
+the same workload (a shorter block of the same cross-section, h, density,
+material and indenter, sized so that the run takes about --ref-seconds).
 """
 import argparse
 import json
@@ -48,7 +50,8 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--ref-seconds", type=float, default=45.0)
+    ap.add_argument("--ref-seconds", type=float, default=45.0,
+                    help="target length of the reference arm's timed part (sizes its per-substep sample)")
     ap.add_argument("--adjoint", action="store_true",
                     help="time the adjoint (forward with checkpoints + reverse sweep) on the calibration workload")
     ap.add_argument("--ckpt-every", type=int, default=20)
@@ -181,7 +184,23 @@ def cpu_baseline(cfg_name, seconds, threads=None):
                       f"(oracle/liboracle.so, FP64, OpenMP {threads} threads)"}
 
 
+def reference_sample(cfg, n_s):
+    """A bounded sample of a block workload: the same cross-section, h, dt,
+    particle density, material, cohesion law and indenter, with the block's
+    length in x (and the grain count of a grains workload) scaled by n_s / n,
+    so the grid shrinks with the particle count."""
+    import dataclasses
+    f = n_s / cfg.n
+    dims = (cfg.dims[0] * f, cfg.dims[1], cfg.dims[2])
+    kw = {"grains": max(1, round(cfg.grains * f))} if cfg.grains else {}
+    return dataclasses.replace(cfg, name=cfg.name + "_sample", n=n_s, dims=dims, **kw)
+
+
 def run_reference(args):
+    """The reference step's CPU port (the oracle, OpenMP on all host cores):
+    exactly --steps substeps, each over a bounded sample of the workload sized
+    from one probe substep of the full block so that the timed part takes
+    about --ref-seconds (the full block when that fits)."""
     world, rank, _ = dist_env()
     if rank != 0:
         return 0
@@ -189,28 +208,40 @@ def run_reference(args):
     from oracle import pyoracle as po
     threads = os.cpu_count() or 1
     cfg = gen.CONFIGS[args.workload]
-    prms, soa, coh = gen.make_block(cfg)
-    n = soa.shape[1]
-    p0 = None if coh is None else coh / prms.DP_tan_phi
-    sim = po.OracleSim(prms, soa, n, p0=p0, svd_mode=0, nthreads=threads)
-    sim.step(max(1, min(args.warmup, 3)))
-    # bounded sample: substeps of the full block until --steps are done or
-    # --ref-seconds have elapsed (a CPU substep of the 8M block takes ~0.4 s)
+
+    def oracle_for(c):
+        prms, soa, coh = gen.make_block(c)
+        n = soa.shape[1]
+        p0 = None if coh is None else coh / prms.DP_tan_phi
+        return po.OracleSim(prms, soa, n, p0=p0, svd_mode=0, nthreads=threads), n
+
+    sim, n_full = oracle_for(cfg)
     t0 = time.perf_counter()
-    done = 0
-    while done < args.steps and (done < 2 or time.perf_counter() - t0 < args.ref_seconds):
-        sim.step(1)
-        done += 1
+    sim.step(1)
+    rate = n_full / (time.perf_counter() - t0)        # probe: particle-substeps/s on this host
+    n_s = min(n_full, max(20_000, int(rate * args.ref_seconds / max(args.steps, 1))))
+    if n_s < n_full:
+        scfg = reference_sample(cfg, n_s)
+        sim, n = oracle_for(scfg)
+        sample = (f"{n} particles per substep: a {scfg.dims[0]:.3f} x {scfg.dims[1]:g} x {scfg.dims[2]:g} m block "
+                  f"of the {cfg.name} workload (same h, dt, density, material, cohesion law, indenter)")
+    else:
+        n = n_full
+        sample = f"the full {n}-particle {cfg.name} block"
+    sim.step(max(1, min(args.warmup, 3)))
+    t0 = time.perf_counter()
+    hist, err = sim.step(args.steps)
     dt = time.perf_counter() - t0
-    value = n * done / dt
+    if err:
+        print(f"reference step reported error code {err}", file=sys.stderr)
+    value = n * args.steps / dt
     out = {"impl": "reference", "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
-           "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / done * 1e3,
+           "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-           "data": "synthetic", "config": {"workload": args.workload, "particles": n},
+           "data": "synthetic", "config": {"workload": args.workload, "particles": n_full},
            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-                            "sample": f"{done} substeps of the full {n}-particle block (oracle port of the "
-                                      f"reference step, FP64, OpenMP {threads} threads; bounded by "
-                                      f"{args.ref_seconds:g} s)"},
+                            "sample": f"{args.steps} substeps of {sample} (oracle port of the reference step, "
+                                      f"FP64, OpenMP {threads} threads)"},
            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return 0
