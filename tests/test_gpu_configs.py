@@ -339,9 +339,15 @@ def test_grains30m_mixed_vs_fp64_and_sorted_keys(grains):
                        ("Jp_inv", slice(IDX_JP_INV, IDX_JP_INV + 1))):
         a, b = field(rows)
         fields[name] = rel(a, b)
+    # C on the lattice block and on the grains (particle ids from n_lat on)
+    n_lat = n - int(round(n * gen.CONFIGS["grains30m"].grain_frac))
+    a, b = field(slice(BP00, BP00 + 9))
+    c_split = (rel(a[:, :n_lat], b[:, :n_lat]), rel(a[:, n_lat:], b[:, n_lat:]))
+    del a, b
     cm, c64 = (crushed(x)[r] for x, r in ((omx, rmx), (o64, r64)))
     flips = int(np.sum(cm != c64))
     print(f"\ngrains30m: {n} particles, {steps} substeps, mixed vs FP64: "
           + ", ".join(f"{k} {v:.2e}" for k, v in fields.items())
+          + f" (block {c_split[0]:.2e}, grains {c_split[1]:.2e})"
           + f", crushed {int(c64.sum())} / flag differences {flips}")
     assert e <= 1e-3
