@@ -29,6 +29,7 @@ class MPMHandle:
         if not self._h:
             raise MPMError(st.value, "mpm_create")
         self.capacity = int(capacity)
+        self._adj_steps = None   # substeps of the last adjoint_forward
 
     def close(self):
         if getattr(self, "_h", None):
@@ -47,11 +48,18 @@ class MPMHandle:
     # -- data
     def upload(self, soa, n=None, cohesion=None):
         soa = np.ascontiguousarray(soa, dtype=np.float64)
-        assert soa.shape[0] == N_PTS_ARRAYS
-        n = soa.shape[1] if n is None else n
-        check(LIB.mpm_upload_soa(self._h, dptr(soa), soa.shape[1], n), "mpm_upload_soa")
+        if soa.ndim != 2 or soa.shape[0] != N_PTS_ARRAYS:
+            raise ValueError(f"soa must have shape ({N_PTS_ARRAYS}, pitch), got {soa.shape}")
+        n = soa.shape[1] if n is None else int(n)
+        if not 0 <= n <= soa.shape[1]:
+            raise ValueError(f"n = {n} outside 0..{soa.shape[1]} (the soa's pitch)")
+        c = None
         if cohesion is not None:
-            c = np.ascontiguousarray(cohesion, dtype=np.float64)
+            c = np.ascontiguousarray(cohesion, dtype=np.float64).ravel()
+            if c.size < n:
+                raise ValueError(f"cohesion holds {c.size} values for {n} particles")
+        check(LIB.mpm_upload_soa(self._h, dptr(soa), soa.shape[1], n), "mpm_upload_soa")
+        if c is not None:
             check(LIB.mpm_upload_cohesion(self._h, dptr(c), n), "mpm_upload_cohesion")
 
     def count(self):
@@ -175,13 +183,19 @@ class MPMHandle:
         """nsteps substeps with a device checkpoint every ckpt_every; returns
         the (nsteps, 3) indenter force history."""
         hist = np.zeros((nsteps, 3))
+        self._adj_steps = None
         check(LIB.mpm_adjoint_forward(self._h, nsteps, ckpt_every, dptr(hist)), "mpm_adjoint_forward")
+        self._adj_steps = int(nsteps)
         return hist
 
     def adjoint_backward(self, dL_dforce):
         """Reverse sweep for dL/d(force history); returns (dL/dcohesion per
         particle in the handle's order, dL/dYoungsModulus)."""
         g = np.ascontiguousarray(dL_dforce, dtype=np.float64).reshape(-1, 3)
+        if self._adj_steps is None:
+            raise MPMError(108, "mpm_adjoint_backward before a successful adjoint_forward")   # MPM_ERR_STATE
+        if g.shape[0] != self._adj_steps:
+            raise ValueError(f"dL_dforce has {g.shape[0]} rows for {self._adj_steps} substeps")
         dc = np.zeros(max(self.count(), 1))
         dE = ctypes.c_double(0.0)
         check(LIB.mpm_adjoint_backward(self._h, dptr(g), dptr(dc), ctypes.byref(dE)), "mpm_adjoint_backward")

@@ -111,3 +111,30 @@ def test_create_rejects_grids_the_kernels_cannot_index():
     assert st.value != 101
     p.GridXTotal, p.GridY, p.GridZ = 1500, 1500, 1000
     assert not LIB.mpm_create(p, 0, 100, 0, ctypes.byref(st)) and st.value == 101
+
+
+def test_python_wrapper_rejects_short_host_arrays_before_the_library_reads_them():
+    """Host-side size checks in MPMHandle: arrays shorter than the counts the
+    library would read raise ValueError before any call crosses the ABI."""
+    import numpy as np
+    import pytest
+    from icempm_3dm_b200 import simulation as sim
+
+    class Fake(sim.MPMHandle):       # no device: only the checks run
+        def __init__(self):
+            self._h = None
+            self._adj_steps = None
+
+    h = Fake()
+    soa = np.zeros((28, 10))
+    with pytest.raises(ValueError):
+        h.upload(np.zeros((27, 10)))
+    with pytest.raises(ValueError):
+        h.upload(soa, n=11)
+    with pytest.raises(ValueError):
+        h.upload(soa, cohesion=np.ones(9))
+    with pytest.raises(sim.MPMError):
+        h.adjoint_backward(np.zeros((5, 3)))
+    h._adj_steps = 4
+    with pytest.raises(ValueError):
+        h.adjoint_backward(np.zeros((5, 3)))
