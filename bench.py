@@ -15,10 +15,12 @@ host buffers (pinned SoA and cohesion uploaded, the cell-key sort, K substeps
 with the force history read back, SoA downloaded) inside the timed region. N > 1 runs independent
 replicas, one per GPU (the path is one partition; no collective).
 
---impl reference times the CPU port of the reference step (the oracle,
-OpenMP on all host cores): exactly K substeps, each over a bounded sample of
-the same workload (a shorter block of the same cross-section, h, density,
-material and indenter, sized so that the run takes about --ref-seconds).
+--impl reference times the reference's own step kernels (mpm_kernels.cuh
+compiled as host C++ from its source into oracle/_ref, OpenMP on all host
+cores; the oracle port when that build is absent), without loading the
+product library: exactly K substeps, each over a bounded sample of the same
+workload (a shorter block of the same cross-section, h, density, material
+and indenter, sized so that the run takes about --ref-seconds).
 """
 import argparse
 import json
@@ -49,6 +51,8 @@ def parse():
     ap.add_argument("--workload", default="block8m")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-arm", action="store_true", help="skip the plain FP64 step on the same block")
+    ap.add_argument("--fp64-steps", type=int, default=300, help="substeps of the FP64 arm (at most --steps)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=45.0,
                     help="target length of the reference arm's timed part (sizes its per-substep sample)")
@@ -161,17 +165,47 @@ def traffic_per_particle(kernel):
     return None
 
 
-def cpu_baseline(cfg_name, seconds, threads=None):
-    """The CPU port of the reference step (oracle, FP64, OpenMP over all host
-    cores) on the same block: warm-up 1 substep, then substeps until
-    `seconds` have elapsed (at least 2)."""
+def reference_cpu(threads):
+    """The reference step on the host cores, without the product library:
+    (make(cfg) -> (sim, n), kind, what). With oracle/_ref/libref_mpm.so (the
+    reference's own mpm_kernels.cuh compiled as host C++ from its source) the
+    sim is oracle.pyoracle.RefSim, kind "reference"; without it, the oracle
+    port (kind "port"). The parameter blocks come from the oracle's own
+    restatement of SimParams3D's routines. The reference kernels have no
+    per-particle cohesion: RefSim runs the workload's median cohesion through
+    the global DP_threshold_p (the same work per particle). The input is
+    sorted by cell key first, as the reference's RemoveDisabledAndSort does
+    after loading."""
     from icempm_3dm_b200 import generator as gen
+    from oracle import params as oracle_params
     from oracle import pyoracle as po
+    use_ref = po.ref_mpm_lib() is not None
+
+    def make(c):
+        prms, soa, coh = gen.make_block(c, ops=oracle_params.OPS)
+        n = soa.shape[1]
+        perm = po.sort_permutation(prms, soa, n)
+        soa = np.ascontiguousarray(soa[:, perm])
+        if use_ref:
+            return po.RefSim(prms, soa, n, nthreads=threads), n
+        p0 = None if coh is None else coh[perm] / prms.DP_tan_phi
+        return po.OracleSim(prms, soa, n, p0=p0, svd_mode=0, nthreads=threads), n
+
+    if use_ref:
+        what = (f"the reference's own mpm_kernels.cuh compiled as host C++ (oracle/_ref/libref_mpm.so), "
+                f"FP64 with its FP32 SVD, OpenMP {threads} threads, median cohesion")
+        return make, "reference", what
+    return make, "port", f"oracle port of the reference step, FP64, OpenMP {threads} threads"
+
+
+def cpu_baseline(cfg_name, seconds, threads=None):
+    """The reference step on the host cores (reference_cpu) on the same
+    block: warm-up 1 substep, then substeps until `seconds` have elapsed (at
+    least 2)."""
+    from icempm_3dm_b200 import generator as gen
     threads = threads or os.cpu_count() or 1
-    prms, soa, coh = gen.make_block(gen.CONFIGS[cfg_name])
-    n = soa.shape[1]
-    p0 = None if coh is None else coh / prms.DP_tan_phi
-    sim = po.OracleSim(prms, soa, n, p0=p0, svd_mode=0, nthreads=threads)
+    make, kind, what = reference_cpu(threads)
+    sim, n = make(gen.CONFIGS[cfg_name])
     sim.step(1)
     t0 = time.perf_counter()
     done = 0
@@ -179,9 +213,8 @@ def cpu_baseline(cfg_name, seconds, threads=None):
         sim.step(1)
         done += 1
     dt = time.perf_counter() - t0
-    return {"value": n * done / dt, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-            "sample": f"{done} substeps of the full {n}-particle block after 1 warm-up substep "
-                      f"(oracle/liboracle.so, FP64, OpenMP {threads} threads)"}
+    return {"value": n * done / dt, "unit": "particle-steps/s", "cores": threads, "kind": kind,
+            "sample": f"{done} substeps of the full {n}-particle block after 1 warm-up substep ({what})"}
 
 
 def reference_sample(cfg, n_s):
@@ -197,32 +230,26 @@ def reference_sample(cfg, n_s):
 
 
 def run_reference(args):
-    """The reference step's CPU port (the oracle, OpenMP on all host cores):
-    exactly --steps substeps, each over a bounded sample of the workload sized
-    from one probe substep of the full block so that the timed part takes
-    about --ref-seconds (the full block when that fits)."""
+    """The reference step on all host cores (reference_cpu; the product
+    library is not loaded): exactly --steps substeps, each over a bounded
+    sample of the workload sized from one probe substep of the full block so
+    that the timed part takes about --ref-seconds (the full block when that
+    fits)."""
     world, rank, _ = dist_env()
     if rank != 0:
         return 0
     from icempm_3dm_b200 import generator as gen
-    from oracle import pyoracle as po
     threads = os.cpu_count() or 1
     cfg = gen.CONFIGS[args.workload]
-
-    def oracle_for(c):
-        prms, soa, coh = gen.make_block(c)
-        n = soa.shape[1]
-        p0 = None if coh is None else coh / prms.DP_tan_phi
-        return po.OracleSim(prms, soa, n, p0=p0, svd_mode=0, nthreads=threads), n
-
-    sim, n_full = oracle_for(cfg)
+    make, kind, what = reference_cpu(threads)
+    sim, n_full = make(cfg)
     t0 = time.perf_counter()
     sim.step(1)
     rate = n_full / (time.perf_counter() - t0)        # probe: particle-substeps/s on this host
     n_s = min(n_full, max(20_000, int(rate * args.ref_seconds / max(args.steps, 1))))
     if n_s < n_full:
         scfg = reference_sample(cfg, n_s)
-        sim, n = oracle_for(scfg)
+        sim, n = make(scfg)
         sample = (f"{n} particles per substep: a {scfg.dims[0]:.3f} x {scfg.dims[1]:g} x {scfg.dims[2]:g} m block "
                   f"of the {cfg.name} workload (same h, dt, density, material, cohesion law, indenter)")
     else:
@@ -239,12 +266,62 @@ def run_reference(args):
            "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic", "config": {"workload": args.workload, "particles": n_full},
-           "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-                            "sample": f"{args.steps} substeps of {sample} (oracle port of the reference step, "
-                                      f"FP64, OpenMP {threads} threads)"},
+           "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": kind,
+                            "sample": f"{args.steps} substeps of {sample} ({what})"},
            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return 0
+
+
+def fp64_arm(args, prms, soa, coh, local, stream, dist, world):
+    """The plain FP64 step (FP64 state and transfers, the reference's FP32
+    SVD) on the same block in the same process: min(--steps, --fp64-steps)
+    substeps after 3 warm-up substeps, CUDA events on the handle's stream, max
+    over ranks; its dominant kernel's roofline from the in-library per-kernel
+    events."""
+    import torch
+    from icempm_3dm_b200 import MPMHandle, PRECISION_FP64
+    n = soa.shape[1]
+    steps = max(1, min(args.steps, args.fp64_steps))
+    device = torch.device("cuda", local)
+    h = MPMHandle(prms, n, PRECISION_FP64, device=local)
+    try:
+        h.set_stream(stream.cuda_stream)
+        h.upload(soa, cohesion=coh)
+        h.sort()
+        h.step(3, want_forces=False)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        h.step(steps)
+        e1.record(stream)
+        e1.synchronize()
+        ms = max_over_ranks(dist, e0.elapsed_time(e1), device)
+        kms = h.step_timed(steps)
+        active = h.active_nodes()
+    finally:
+        h.close()
+    names = ["grid clear", "k_p2g_pairs_f64", "k_update_f64", "k_g2p_f64"]
+    k = int(np.argmax(kms[1:])) + 1
+    dom_ms = kms[k] / steps
+    # FP64 form: P2G reads 200 B (utility, x, v, F, C) and writes the grid
+    # (32 B per active node); G2P reads 112 B (+ 8 B cohesion) and the grid
+    # (32 B per node), writes 208 B
+    per = {1: 200, 3: 320 + (8 if coh is not None else 0)}.get(k, 0)
+    dom_bytes = n * per + active * 32
+    peak, peak_kind = measured_peak_hbm()
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    step_bytes = n * (B_PARTICLE["fp64"] + (B_COHESION["fp64"] if coh is not None else 0)) + active * B_NODE["fp64"]
+    return {"value": world * n * steps / (ms * 1e-3), "unit": "particle-steps/s", "steps": steps,
+            "ms_per_step": ms / steps, "dtype": "f64",
+            "kernel_ms_per_step": {"clear": kms[0] / steps, "p2g": kms[1] / steps, "update": kms[2] / steps,
+                                   "g2p": kms[3] / steps},
+            "hbm_fraction_step": step_bytes / (ms / steps * 1e-3) / 1e9 / peak,
+            "roofline": {"bound": "hbm", "kernel": names[k], "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak}}
 
 
 def run_ours(args):
@@ -307,8 +384,9 @@ def run_ours(args):
         names = ["grid clear", "k_p2g_pairs_f64", "k_update_f64", "k_g2p_f64"]
         k = int(np.argmax(kms[1:])) + 1
         dom_name, dom_ms = names[k], kms[k] / args.steps
-        # FP64 form: P2G reads 200 B (x, v, F, C), G2P reads 112 B and writes 208 B
-        per = {1: 200, 3: 320}.get(k, 0)
+        # FP64 form: P2G reads 200 B (utility, x, v, F, C), G2P reads 112 B
+        # (+ 8 B cohesion) and writes 208 B
+        per = {1: 200, 3: 320 + (8 if coh is not None else 0)}.get(k, 0)
         dom_bytes = n * per + (active * 32 if k in (1, 3) else active * 64)
         launches_per_step = 3
     peak, peak_kind = measured_peak_hbm()
@@ -350,6 +428,11 @@ def run_ours(args):
            "d2h_bytes_per_step": (soa.nbytes + 24 * args.steps) / args.steps,
            "calls": "mpm_upload_soa + mpm_upload_cohesion + mpm_sort + mpm_step(K) + mpm_download_soa"}
 
+    # --- the plain FP64 step on the same block (the "mixed vs FP64" ratio)
+    fp64 = None
+    if prec == PRECISION_MIXED and not args.no_fp64_arm:
+        fp64 = fp64_arm(args, prms, soa, coh, local, stream, dist, world)
+
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(args.workload, args.cpu_seconds)
@@ -375,7 +458,7 @@ def run_ours(args):
                                    {"update": kms[2] / args.steps, "g2p": kms[3] / args.steps,
                                     "p2g": kms[1] / args.steps, "clear": kms[0] / args.steps}),
             "force_last": hist[-1].tolist(),
-            "cpu_baseline": base, "e2e": e2e, "clocks": clocks,
+            "fp64": fp64, "cpu_baseline": base, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches_per_step * args.steps,
         }
         print(json.dumps(out), flush=True)

@@ -66,17 +66,19 @@ def build_library(force=False, verbose=False):
 
 
 def build_oracle():
-    """The CPU oracle (test infrastructure) and, where the reference tree is
-    present, its compiled reference SVD under oracle/_ref."""
+    """The CPU oracle (test infrastructure) and its `ref` target: the
+    reference's own SVD and step kernels under oracle/_ref, built by
+    oracle/Makefile from the reference tree when that tree is present (the
+    Makefile names its default location; ICEMPM_REFERENCE_TREE overrides
+    it)."""
     odir = os.path.join(ROOT, "oracle")
     r = subprocess.run(["make", "-C", odir], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
-    ref = os.environ.get("ICEMPM_REFERENCE_TREE", "/root/reference")
-    if os.path.isdir(os.path.join(ref, "simulation")):
-        r = subprocess.run(["make", "-C", odir, "ref", f"REF={ref}"], capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError("oracle/_ref build failed:\n" + r.stdout + r.stderr)
+    ref = os.environ.get("ICEMPM_REFERENCE_TREE")
+    r = subprocess.run(["make", "-C", odir, "ref"] + ([f"REF={ref}"] if ref else []), capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle/_ref build failed:\n" + r.stdout + r.stderr)
 
 
 if __name__ == "__main__":

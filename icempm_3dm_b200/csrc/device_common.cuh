@@ -11,7 +11,7 @@ namespace icempm {
 
 // The subset of SimParams3D the kernels read, with derived constants, passed
 // by value as a kernel argument (the reference copies the whole struct to a
-// __constant__ symbol, gpu_partition_3d.cu:306; a by-value argument lives in
+// __constant__ symbol, gpu_partition_3d.cu:140; a by-value argument lives in
 // the same constant bank and keeps handles independent).
 struct DevParams {
     int Gx, Gy, Gz, halo;          // GridXTotal, GridY, GridZ, GridHaloSize

@@ -13,13 +13,29 @@ LoadRawPoints does:
     y = block_top + r - IndDepth (snapshotmanager.cpp:82-96);
   - ParticleVolume = Volume / N (:99).
 Per-particle cohesion (lognormal) is drawn from the same RNG.
+
+The parameter block's defaults and derived constants come from a set of
+SimParams3D routines, `ops` (Reset, SetPhi, ComputeCamClayParams,
+ComputeHelperVariables): by default the library's own (mpm_params_*); any
+other set with the same meaning can be passed. This module loads the library
+only when the default set is used.
 """
 import dataclasses
 import math
+from collections import namedtuple
 
 import numpy as np
 
-from ._lib import (FE00, IDX_JP_INV, LIB, N_PTS_ARRAYS, POSX, SimParams3D)
+from .layout import FE00, IDX_JP_INV, N_PTS_ARRAYS, POSX, SimParams3D
+
+ParamOps = namedtuple("ParamOps", "reset set_phi compute_camclay compute_helper_variables")
+
+
+def library_param_ops():
+    """The library's SimParams3D routines (include/icempm_b200.h)."""
+    from ._lib import LIB
+    return ParamOps(LIB.mpm_params_reset, LIB.mpm_params_set_phi, LIB.mpm_params_compute_camclay,
+                    LIB.mpm_params_compute_helper_variables)
 
 _M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
 
@@ -135,11 +151,13 @@ def grid_dims(cfg):
     return gx, gy, gz
 
 
-def make_params(cfg, n=None):
-    """SimParams3D for cfg; derived constants via the library's own
-    ComputeCamClayParams / ComputeHelperVariables."""
+def make_params(cfg, n=None, ops=None):
+    """SimParams3D for cfg; defaults and derived constants by ops.reset /
+    ops.compute_camclay / ops.compute_helper_variables (default: the
+    library's own)."""
+    ops = ops or library_param_ops()
     p = SimParams3D()
-    LIB.mpm_params_reset(p)
+    ops.reset(p)
     gx, gy, gz = grid_dims(cfg)
     p.GridXTotal, p.GridY, p.GridZ = gx, gy, gz
     p.DomainDimensionX = gx * cfg.h
@@ -149,7 +167,7 @@ def make_params(cfg, n=None):
     p.YoungsModulus = cfg.youngs
     p.PoissonsRatio = cfg.poisson
     p.Density = cfg.density
-    LIB.mpm_params_set_phi(p, cfg.phi_deg)
+    ops.set_phi(p, cfg.phi_deg)
     p.DP_threshold_p = cfg.cohesion_median / p.DP_tan_phi
     p.GrainVariability = 0.0
     p.IndDiameter = 2 * cfg.ind_radius
@@ -157,23 +175,25 @@ def make_params(cfg, n=None):
     p.IndDepth = cfg.ind_radius
     p.nPtsTotal = cfg.n if n is None else n
     p.Volume = float(np.prod(cfg.dims))
-    LIB.mpm_params_compute_camclay(p)
-    LIB.mpm_params_compute_helper_variables(p)
+    ops.compute_camclay(p)
+    ops.compute_helper_variables(p)
     return p
 
 
-def make_block(cfg, n=None):
+def make_block(cfg, n=None, ops=None):
     """(prms, soa, cohesion): soa is a (28, n) float64 host SoA in the
-    reference layout; cohesion is None for uniform cohesion."""
+    reference layout; cohesion is None for uniform cohesion. ops: the
+    SimParams3D routines (default: the library's)."""
+    ops = ops or library_param_ops()
     if cfg.grains > 0:
-        return make_grains_block(cfg, n)
+        return make_grains_block(cfg, n, ops)
     n = cfg.n if n is None else n
     dims = cfg.dims
     if n != cfg.n:   # a smaller copy of the same block keeps the spacing
         scale = (n / cfg.n) ** (1.0 / 3.0)
         dims = tuple(d * scale for d in cfg.dims)
         cfg = dataclasses.replace(cfg, dims=dims, n=n)
-    p = make_params(cfg, n)
+    p = make_params(cfg, n, ops)
     pos = jittered_lattice(n, dims, cfg.seed)
     h = p.cellsize
     mins, maxs = pos.min(axis=1), pos.max(axis=1)
@@ -196,7 +216,7 @@ def make_block(cfg, n=None):
     p.indenter_x_initial = p.indenter_x
     p.indenter_y_initial = p.indenter_y
     p.ParticleVolume = p.Volume / n
-    LIB.mpm_params_compute_helper_variables(p)
+    ops.compute_helper_variables(p)
 
     soa = np.zeros((N_PTS_ARRAYS, n), dtype=np.float64)
     soa[POSX:POSX + 3] = pos
@@ -210,7 +230,7 @@ def make_block(cfg, n=None):
     return p, soa, cohesion
 
 
-def make_grains_block(cfg, n=None):
+def make_grains_block(cfg, n=None, ops=None):
     """The non-uniform stress case: (1 - grain_frac) of the particles on a
     jittered lattice filling the lower block_frac_y of the domain (placed as
     make_block places a block), grain_frac of them in cfg.grains spheres with
@@ -219,6 +239,7 @@ def make_grains_block(cfg, n=None):
     of those particles proportional to its volume, spread uniformly inside it.
     Every particle has the lattice's particle volume. A smaller n scales the
     domain and the grain count with the particle count."""
+    ops = ops or library_param_ops()
     n = cfg.n if n is None else n
     if n != cfg.n:
         scale = (n / cfg.n) ** (1.0 / 3.0)
@@ -228,7 +249,7 @@ def make_grains_block(cfg, n=None):
     n_lat = n - n_grain
     dom = np.asarray(cfg.dims, dtype=np.float64)
     lat_dims = (dom[0], dom[1] * cfg.block_frac_y, dom[2])
-    p = make_params(cfg, n)
+    p = make_params(cfg, n, ops)
     h = p.cellsize
     lat = jittered_lattice(n_lat, lat_dims, cfg.seed)
     box_x, box_z = p.GridXTotal * h, p.GridZ * h
@@ -270,7 +291,7 @@ def make_grains_block(cfg, n=None):
     p.indenter_y_initial = p.indenter_y
     p.Volume = float(np.prod(lat_dims)) * n / n_lat
     p.ParticleVolume = float(np.prod(lat_dims)) / n_lat
-    LIB.mpm_params_compute_helper_variables(p)
+    ops.compute_helper_variables(p)
 
     soa = np.zeros((N_PTS_ARRAYS, n), dtype=np.float64)
     soa[POSX:POSX + 3] = pos
@@ -283,11 +304,11 @@ def make_grains_block(cfg, n=None):
 
 
 def small_block(n=4000, seed=5, dims=(0.2, 0.1, 0.1), h=0.01, dt=1e-5, ind_velocity=0.2,
-                cohesion_sigma_log=0.0, youngs=5e8):
+                cohesion_sigma_log=0.0, youngs=5e8, halo=0, ops=None):
     """A small block for parity tests (seconds on the oracle)."""
     cfg = BlockConfig("small", n, dims, h, seed, dt, 0, ind_velocity, cohesion_sigma_log=cohesion_sigma_log,
-                      youngs=youngs)
-    return make_block(cfg)
+                      youngs=youngs, halo=halo)
+    return make_block(cfg, ops=ops)
 
 
 def calibration_block(n=20_000, penetration_cells=3, ind_velocity=2.0, cohesion_sigma_log=0.3):
@@ -304,6 +325,6 @@ def calibration_block(n=20_000, penetration_cells=3, ind_velocity=2.0, cohesion_
     return prms, soa, coh
 
 
-__all__ = ["BlockConfig", "CONFIGS", "make_block", "make_grains_block", "make_params", "small_block",
-           "calibration_block",
+__all__ = ["BlockConfig", "CONFIGS", "ParamOps", "library_param_ops", "make_block", "make_grains_block",
+           "make_params", "small_block", "calibration_block",
            "jittered_lattice", "splitmix64", "uniform", "normal"]

@@ -221,7 +221,8 @@ class GPU_Implementation6:
         self.indenter_force = np.zeros(3)
         self.indenter_sensor_total = None
 
-    # initialize + allocate_arrays + update_constants (gpu_implementation6.cpp:380-462, 583)
+    # GPU_Implementation6::initialize (gpu_implementation6.cpp:319-337), allocate_arrays (:385-401),
+    # update_constants (:522-525)
     def initialize(self, capacity):
         self.handle = MPMHandle(self.prms, capacity, self.precision, self.device)
 

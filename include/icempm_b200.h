@@ -50,9 +50,12 @@ extern "C" {
 
 #define MPM_PRECISION_FP64   0    /* FP64 state and transfers; 3x3 SVD in FP32
                                      exactly as the reference (helper_math.cuh) */
-#define MPM_PRECISION_MIXED  1    /* FP32 state and transfers, fixed-point grid
-                                     accumulation; FP64 SVD, apex return map and
-                                     indenter force reduction                 */
+#define MPM_PRECISION_MIXED  1    /* FP32 state and transfers; the grid is
+                                     accumulated with plain FP32 float4
+                                     atomics (same-cell particle pairs merged
+                                     in registers first): no compensated or
+                                     fixed-point sum; FP64 SVD, apex return
+                                     map and indenter force reduction        */
 #define MPM_PRECISION_FP64_SVD64 2 /* FP64 throughout, SVD included: the
                                      high-accuracy reference of the mixed mode */
 
@@ -82,9 +85,12 @@ int  mpm_params_parse_string(SimParams3D* prms, const char* json_text,
 
 /* ---------------------------------------------------------------- handle */
 
-/* GPU_Implementation6::initialize + allocate_arrays + update_constants
- * (gpu_implementation6.cpp:380-398, 446-462, 583-586;
- *  gpu_partition_3d.cu:218-309). One partition on `device`.
+/* GPU_Implementation6::initialize (gpu_implementation6.cpp:319-337),
+ * GPU_Implementation6::allocate_arrays (:385-401),
+ * GPU_Implementation6::update_constants (:522-525) and
+ * GPU_Partition_3D::initialize (gpu_partition_3d.cu:52-73),
+ * GPU_Partition_3D::allocate (:76-132), GPU_Partition_3D::update_constants
+ * (:135-143). One partition on `device`.
  * `capacity` = number of particles the handle can hold. The grid is the
  * reference's one-partition buffer, (GridXTotal + 2 GridHaloSize) x GridY x
  * GridZ nodes (GridHaloSize = 0 needs no halo slabs with one partition),
@@ -94,30 +100,33 @@ int  mpm_params_parse_string(SimParams3D* prms, const char* json_text,
  * *status receives 0 or an error code; NULL is returned on error. */
 mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity,
                        int device, int* status);
-/* ~GPU_Partition_3D (gpu_partition_3d.cu:193-216). */
+/* GPU_Partition_3D::~GPU_Partition_3D (gpu_partition_3d.cu:27-50). */
 void mpm_destroy(mpm_handle* h);
 /* Issue all later work of h on `cuda_stream` (a cudaStream_t); NULL restores
  * the handle's own stream. */
 int  mpm_set_stream(mpm_handle* h, void* cuda_stream);
-/* GPU_Implementation6::update_constants (gpu_implementation6.cpp:583-586;
- * gpu_partition_3d.cu:301-309): copies the parameter block to the device and
- * clears the device error byte. The grid dimensions must not change. */
+/* GPU_Implementation6::update_constants (gpu_implementation6.cpp:522-525),
+ * GPU_Partition_3D::update_constants (gpu_partition_3d.cu:135-143): copies
+ * the parameter block to the device and clears the device error byte. The
+ * grid dimensions must not change. */
 int  mpm_update_constants(mpm_handle* h, const SimParams3D* prms);
 
 /* -------------------------------------------------------- particle data */
 
-/* GPU_Implementation6::transfer_ponts_to_device (gpu_implementation6.cpp:465-475;
- * gpu_partition_3d.cu:367-381): n particles from a host SoA in the
- * reference's HostSideSOA row layout (row k at soa + k*pitch, 28 rows). */
+/* GPU_Implementation6::transfer_ponts_to_device (gpu_implementation6.cpp:404-414),
+ * GPU_Partition_3D::transfer_points_from_soa_to_device (gpu_partition_3d.cu:201-215):
+ * n particles from a host SoA in the reference's HostSideSOA row layout
+ * (row k at soa + k*pitch, 28 rows). */
 int  mpm_upload_soa(mpm_handle* h, const double* soa, unsigned pitch, unsigned n);
 /* New per-particle field (no reference counterpart): cohesion c_i in Pa.
  * The Drucker-Prager apex shift becomes p0_i = c_i / DP_tan_phi in place of
  * the global DP_threshold_p (mpm_kernels.cuh:499,505-509,525). NULL clears
  * the field and restores the global value. */
 int  mpm_upload_cohesion(mpm_handle* h, const double* cohesion, unsigned n);
-/* GPU_Implementation6::transfer_from_device (gpu_implementation6.cpp:478-557;
- * gpu_partition_3d.cu:335-365): writes the particles in the handle's current
- * order into the host SoA (28 rows, row stride pitch >= n), *n = count.
+/* GPU_Implementation6::transfer_from_device (gpu_implementation6.cpp:417-496),
+ * GPU_Partition_3D::transfer_from_device (gpu_partition_3d.cu:169-199):
+ * writes the particles in the handle's current order into the host SoA
+ * (28 rows, row stride pitch >= n), *n = count.
  * Returns the device error code (70..75) if one was raised, as the
  * reference throws on it. */
 int  mpm_download_soa(mpm_handle* h, double* soa, unsigned pitch, unsigned* n);
@@ -172,18 +181,19 @@ int  mpm_reset_grid(mpm_handle* h);
 /* GPU_Implementation6::p2g (gpu_implementation6.cpp:31-77). */
 int  mpm_p2g(mpm_handle* h);
 /* GPU_Implementation6::update_nodes (gpu_implementation6.cpp:115-123); the
- * indenter centre is passed by value as in gpu_partition_3d.cu:416-419. */
+ * indenter centre is passed by value as GPU_Partition_3D::update_nodes
+ * (gpu_partition_3d.cu:243-255) passes it. */
 int  mpm_update_nodes(mpm_handle* h, double indenter_x, double indenter_y);
 /* GPU_Implementation6::g2p (gpu_implementation6.cpp:125-133); record_pq as
  * recordPQ (mpm_kernels.cuh:347-351). */
 int  mpm_g2p(mpm_handle* h, int record_pq);
-/* GPU_Implementation6::reset_indenter_force_accumulator
- * (gpu_implementation6.cpp:527; gpu_partition_3d.cu:311-316). */
+/* GPU_Implementation6::reset_indenter_force_accumulator (gpu_implementation6.cpp:527-534),
+ * GPU_Partition_3D::reset_indenter_force_accumulator (gpu_partition_3d.cu:145-150). */
 int  mpm_reset_indenter_force_accumulator(mpm_handle* h);
 
 /* ---------------------------------------------------------------- driver */
 
-/* The substep loop of Model3D::Step (model_3d.cpp:35-51) for nsteps
+/* The substep loop of Model3D::Step (model_3d.cpp:24-112, the loop at :35-51) for nsteps
  * substeps: SimulationTime += dt; indenter_x = indenter_x_initial +
  * SimulationTime*IndVelocity; reset grid, P2G, grid update, G2P (P,Q
  * recorded when SimulationStep % UpdateEveryNthStep == 0);
@@ -192,15 +202,16 @@ int  mpm_reset_indenter_force_accumulator(mpm_handle* h);
  * sensor bins of that substep, N). Returns the device error code if one was
  * raised during these substeps. */
 int  mpm_step(mpm_handle* h, int nsteps, double* force_hist);
-/* The frame-level sensor readout of transfer_from_device
- * (gpu_implementation6.cpp:499-520): sensor receives
+/* The frame-level sensor readout of GPU_Implementation6::transfer_from_device
+ * (gpu_implementation6.cpp:417-496, the sensor at :438-459): sensor receives
  * 3*IndenterSubdivisions*GridZ doubles, each divided by
  * UpdateEveryNthStep*cellsize^2; total receives the summed force divided by
- * UpdateEveryNthStep (evaluate_indenter_total_force, :560-571). */
+ * UpdateEveryNthStep (GPU_Implementation6::evaluate_indenter_total_force,
+ * gpu_implementation6.cpp:499-510). */
 int  mpm_sensors(mpm_handle* h, double* sensor, double total[3]);
 /* The device error byte (gpu_error_indicator, mpm_kernels.cuh:17). */
 int  mpm_get_error(mpm_handle* h);
-/* GPU_Implementation6::synchronize (gpu_implementation6.cpp:574-581). */
+/* GPU_Implementation6::synchronize (gpu_implementation6.cpp:513-520). */
 int  mpm_synchronize(mpm_handle* h);
 /* Read back the handle's copy of the parameter block (SimulationTime,
  * SimulationStep, indenter_x advance inside mpm_step). */
@@ -246,14 +257,20 @@ int  mpm_adjoint(mpm_handle* h, int nsteps, int ckpt_every, const double* dL_dfo
  * scratch is a fixed array of about 10 MB compiled into the library, held by
  * every GPU that loads it until the process exits, which limits a call to
  * n <= 524,288 particles and (GridXTotal + 2*GridHaloSize + 1)*GridY*GridZ + 1
- * <= 1,048,576 cell keys (MPM_ERR_NOALLOC_LIMIT beyond). The first call on a
- * device looks up that array's device address there (with the device
- * current); make that first call before any stream capture. Work is issued
- * on `stream` (a cudaStream_t, NULL = legacy default) on the current device,
- * and the call waits for it. All calls share the one array: calls that
- * overlap on the GPU (other host threads, other streams) race and must be
- * serialised by the caller. Returns 0, 107 if a key falls outside the grid,
- * or an error code. */
+ * <= 1,048,576 cell keys (MPM_ERR_NOALLOC_LIMIT beyond, checked before any
+ * device work). The first call on a device looks up that array's device
+ * address there (with the device current) and keeps it for the life of the
+ * process: make that first call before any stream capture, and make no call
+ * after a cudaDeviceReset of that device or from a context other than the
+ * device's primary context (the kept address then belongs to a context that
+ * no longer exists or is not current). Work is issued on `stream` (a
+ * cudaStream_t, NULL = legacy default) on the current device, and the call
+ * waits for it. All calls share the one array: calls that overlap on the GPU
+ * (other host threads, other streams) race and must be serialised by the
+ * caller. Returns 0; MPM_ERR_SORT_RANGE (107) if a particle's cell key falls
+ * outside the grid, in which case the contents of perm and *kept are
+ * unspecified and must not be used (the next call clears the error and
+ * sorts normally); or another error code. */
 int  mpm_sort_permutation_noalloc(const SimParams3D* prms, const double* soa, unsigned pitch,
                                   unsigned n, unsigned* perm, unsigned* kept, void* stream);
 /* Text of the last CUDA failure seen by this thread (MPM_ERR_CUDA). */

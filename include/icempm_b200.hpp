@@ -8,7 +8,7 @@
  *                        std::vector
  *   GPU_Implementation6  gpu_implementation6.h:24-59 for one partition: the
  *                        halo and point-transfer methods do nothing
- *   Model3D              model_3d.h:26-58 / model_3d.cpp:24-112: Reset,
+ *   Model3D              model_3d.h:30-55 / model_3d.cpp:24-112: Reset,
  *                        Prepare, Step (one frame of UpdateEveryNthStep
  *                        substeps through the phase API)
  *

@@ -182,3 +182,117 @@ class OracleSim:
             if e and not err:
                 err = e
         return hist, err
+
+
+# ------------------------------------------------------------------------
+# The reference's own step kernels (oracle/_ref/libref_mpm.so: mpm_kernels.cuh
+# compiled as host C++ from the reference tree, see oracle/ref_kernels.cpp)
+
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def ref_mpm_lib():
+    """The reference's own kernels compiled on the host, or None if not built."""
+    path = os.path.join(_HERE, "_ref", "libref_mpm.so")
+    if not os.path.exists(path):
+        return None
+    lib = ctypes.CDLL(path)
+    lib.ref_sizeof_params.restype = ctypes.c_size_t
+    lib.ref_params_layout.argtypes = [ctypes.POINTER(ctypes.c_size_t)]
+    lib.ref_set_params.restype = ctypes.c_int
+    lib.ref_set_params.argtypes = [ctypes.c_void_p, ctypes.c_size_t]
+    lib.ref_error.restype = ctypes.c_int
+    lib.ref_p2g.argtypes = [ctypes.c_int] * 5 + [_dp, _dp, ctypes.c_int]
+    lib.ref_receive_halos.argtypes = [ctypes.c_int] * 3 + [_dp, _dp, _dp]
+    lib.ref_update_nodes.argtypes = [ctypes.c_double, ctypes.c_double] + [ctypes.c_int] * 3 + [_dp, _dp,
+                                                                                                  ctypes.c_int]
+    lib.ref_g2p.argtypes = [ctypes.c_int] * 7 + [_dp, _dp, _ip, ctypes.c_int, _dp, _dp, ctypes.c_int]
+    lib.ref_receive_points.argtypes = [ctypes.c_int] * 3 + [_dp, _dp]
+    return lib
+
+
+def reference_tree():
+    """The reference source tree oracle/_ref was built from (its Makefile
+    records the path), or None when that tree is not on this machine."""
+    try:
+        with open(os.path.join(_HERE, "_ref", "reference_tree")) as f:
+            path = f.read().strip()
+    except OSError:
+        return None
+    return path if os.path.isdir(os.path.join(path, "simulation")) else None
+
+
+class RefSim:
+    """Substeps of Model3D::Step (model_3d.cpp:35-51) for one partition,
+    driven as GPU_Implementation6 drives its partition (reset_grid, p2g,
+    update_nodes, g2p; gpu_implementation6.cpp:18-133,
+    gpu_partition_3d.cu:222-292), through the reference's own kernels.
+
+    nthreads <= 1 runs each kernel serially in index order (deterministic);
+    more runs it over OpenMP threads. The grid is one partition's buffer of
+    4 arrays of (GridXTotal + 2 GridHaloSize) GridY GridZ doubles (the
+    halo-transfer slabs of gpu_partition_3d.cu:88-95 are not needed with one
+    partition). force of a substep = the sum of that substep's sensor bins.
+    """
+
+    def __init__(self, prms, soa, n, nthreads=1):
+        import copy
+        lib = ref_mpm_lib()
+        if lib is None:
+            raise RuntimeError("oracle/_ref/libref_mpm.so is not built (make -C oracle ref)")
+        self.lib = lib
+        self.prms = copy.copy(prms)
+        self.soa = np.array(soa, dtype=np.float64, copy=True, order="C")
+        self.n = n
+        self.nthreads = nthreads
+        P = self.prms
+        self.nodes = (P.GridXTotal + 2 * P.GridHaloSize) * P.GridY * P.GridZ
+        self.grid = np.zeros((4, self.nodes))
+        self.sensor = np.zeros(3 * P.IndenterSubdivisions * P.GridZ)
+        self.step_sensor = np.zeros_like(self.sensor)
+        cap = max(int(P.VectorCapacity_transfer), 1)
+        self.cap = cap
+        self.xfer = [np.zeros(cap * 28), np.zeros(cap * 28)]
+        self.utility = np.zeros(3, dtype=np.int32)
+        self.count_unupdated = 0
+
+    def _upload_params(self):
+        if self.lib.ref_set_params(ctypes.byref(self.prms), ctypes.sizeof(self.prms)) != 0:
+            raise RuntimeError("SimParams3D layout differs from the reference's")
+
+    def p2g(self):
+        P = self.prms
+        self.lib.ref_p2g(P.GridXTotal, 0, self.nodes, self.n, self.soa.shape[1], _ptr(self.soa), _ptr(self.grid),
+                         self.nthreads)
+
+    def update_nodes(self, ind_x, ind_y):
+        self.step_sensor[:] = 0
+        self.lib.ref_update_nodes(ind_x, ind_y, self.nodes, 0, self.nodes, _ptr(self.grid),
+                                  _ptr(self.step_sensor), self.nthreads)
+        self.sensor += self.step_sensor
+        return self.step_sensor.reshape(-1, 3).sum(axis=0)
+
+    def g2p(self, record_pq, enable_transfer=False):
+        P = self.prms
+        self.utility[:] = 0
+        self.lib.ref_g2p(int(record_pq), int(enable_transfer), P.GridXTotal, 0, self.nodes, self.n,
+                         self.soa.shape[1], _ptr(self.soa), _ptr(self.grid), _ptr(self.utility, _ip), self.cap,
+                         _ptr(self.xfer[0]), _ptr(self.xfer[1]), self.nthreads)
+
+    def step(self, nsteps=1):
+        """nsteps substeps; returns (force history [nsteps, 3], error byte)."""
+        P = self.prms
+        self._upload_params()
+        hist = np.zeros((nsteps, 3))
+        t = P.SimulationTime
+        for s in range(nsteps):
+            t += P.InitialTimeStep
+            P.indenter_x = P.indenter_x_initial + t * P.IndVelocity
+            self.grid[:] = 0
+            self.p2g()
+            hist[s] = self.update_nodes(P.indenter_x, P.indenter_y)
+            is_zero = (P.SimulationStep + s) % P.UpdateEveryNthStep == 0
+            self.g2p(is_zero)
+        P.SimulationTime = t
+        P.SimulationStep += nsteps
+        return hist, self.lib.ref_error()

@@ -4,7 +4,7 @@ branches of the step."""
 import numpy as np
 
 from icempm_3dm_b200 import generator as gen
-from icempm_3dm_b200._lib import (BP00, FE00, IDX_JP_INV, IDX_UTILITY, STATUS_CRUSHED,
+from icempm_3dm_b200.layout import (BP00, FE00, IDX_JP_INV, IDX_UTILITY, STATUS_CRUSHED,
                                   STATUS_LIQUID, VELX)
 
 
@@ -17,11 +17,13 @@ def util_bits(soa):
 
 
 def perturbed_block(n=3000, seed=11, crushed_frac=0.15, strong_frac=0.1, tension_frac=0.03, liquid_frac=0.0,
-                    dims=(0.2, 0.1, 0.1), h=0.01, ind_velocity=0.2):
+                    dims=(0.2, 0.1, 0.1), h=0.01, ind_velocity=0.2, youngs=5e8, ops=None):
     """A small block whose particles carry velocity, affine velocity and
     elastic strain; some are pre-crushed, some strongly strained, a few in
-    tension with Jp_inv < 1."""
-    prms, soa, _ = gen.small_block(n=n, seed=seed, dims=dims, h=h, ind_velocity=ind_velocity)
+    tension with Jp_inv < 1. ops: the SimParams3D routines of the generator
+    (default: the library's)."""
+    prms, soa, _ = gen.small_block(n=n, seed=seed, dims=dims, h=h, ind_velocity=ind_velocity, youngs=youngs,
+                                   ops=ops)
     n = soa.shape[1]
     rng = np.random.default_rng(seed)
     soa[VELX:VELX + 3] = 0.05 * rng.standard_normal((3, n))

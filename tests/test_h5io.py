@@ -16,8 +16,10 @@ import pytest
 
 from icempm_3dm_b200 import h5io
 
-REF_H5 = os.path.join(os.environ.get("ICEMPM_REFERENCE_TREE", "/root/reference"),
-                      "build", "geometries_3d", "3d_200k.h5")
+from oracle import pyoracle as po  # noqa: E402
+
+# the tree oracle/_ref was built from, if it is on this machine
+REF_H5 = os.path.join(po.reference_tree() or "", "build", "geometries_3d", "3d_200k.h5")
 needs_ref = pytest.mark.skipif(not os.path.exists(REF_H5), reason="reference point cloud not present")
 
 

@@ -89,7 +89,9 @@ def test_parse_file_and_errors(tmp_path):
 
 
 def test_reference_input_files_parse_when_present():
-    files = sorted(glob.glob("/root/reference/input_data/*.json"))
+    from oracle import pyoracle as po
+    ref = po.reference_tree()
+    files = sorted(glob.glob(os.path.join(ref, "input_data", "*.json"))) if ref else []
     if not files:
         pytest.skip("reference tree not present")
     for path in files:

@@ -14,7 +14,9 @@ from icempm_3dm_b200 import generator as gen
 from icempm_3dm_b200._lib import FE00, IDX_JP_INV, IDX_UTILITY, LIB, N_PTS_ARRAYS, POSX
 from icempm_3dm_b200.h5io import H5File
 
-REF = os.environ.get("ICEMPM_REFERENCE_TREE", "/root/reference")
+from oracle import pyoracle as po  # noqa: E402
+
+REF = po.reference_tree() or ""          # the tree oracle/_ref was built from, if on this machine
 P1 = os.path.join(REF, "input_data", "p1.json")
 PC = os.path.join(REF, "build", "geometries_3d", "3d_200k.h5")
 needs_ref = pytest.mark.skipif(not (os.path.exists(P1) and os.path.exists(PC)), reason="reference inputs not present")
