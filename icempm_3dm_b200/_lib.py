@@ -60,13 +60,10 @@ ENTRY_POINTS = [
     ("mpm_adjoint", ctypes.c_int, [_hp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp]),
     ("mpm_sort_permutation_noalloc", ctypes.c_int,
      [_pp, ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p, _up, ctypes.c_void_p]),
-    ("mpm_testing_set_p2g_variant", ctypes.c_int, [_hp, ctypes.c_int]),
-    ("mpm_testing_set_g2p_variant", ctypes.c_int, [_hp, ctypes.c_int]),
     ("mpm_testing_svd3x3", ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int]),
     ("mpm_testing_sizeof_params", ctypes.c_size_t, []),
     ("mpm_testing_step_timed", ctypes.c_int, [_hp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
     ("mpm_testing_active_nodes", ctypes.c_int, [_hp, ctypes.POINTER(ctypes.c_longlong)]),
-    ("mpm_testing_copy_wait_timeout", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     ("mpm_testing_download_grid", ctypes.c_int, [_hp, _dp, ctypes.c_int]),
 ]
 

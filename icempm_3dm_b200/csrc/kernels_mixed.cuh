@@ -319,204 +319,6 @@ __device__ __forceinline__ void g2p_gather_staged(const DevParams& P, const floa
     __syncwarp();
 }
 
-// ------------------------------------------------- TMA-staged gather box
-// The velocity grid as a 4-D tensor (float components, z, y, x): one tensor
-// copy brings a fixed box of kTmaBoxX x kTmaBoxY x kTmaBoxZ nodes (4,608 B,
-// innermost coordinate 0, so always 16-byte aligned) into the warp's shared
-// slice, completed on a per-warp mbarrier. Plain (non-multicast) loads.
-constexpr int kTmaBoxX = 3, kTmaBoxY = 3, kTmaBoxZ = 20;
-constexpr int kTmaBoxNodes = kTmaBoxX * kTmaBoxY * kTmaBoxZ;
-constexpr unsigned kTmaBoxBytes = kTmaBoxNodes * 16u;
-constexpr int kTmaSliceNodes = 184;   // per-warp slice: >= kTmaBoxNodes, a multiple of 128 B
-constexpr int kTmaWaitPolls = 1 << 22;   // polls of one bounded wait (a copy takes ~1 us)
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init_one(unsigned long long* bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait for phase `parity` of bar: false when `polls` polls passed.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
-                                                  int polls = kTmaWaitPolls) {
-    for (int k = 0; k < polls; k++)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-
-// Test of the bounded wait's error path: one warp arms an mbarrier for 16
-// bytes that no copy delivers (nothing is in flight), waits at most `polls`
-// polls and records MPM_ERR_COPY_TIMEOUT, or 0 if the phase completed.
-__global__ void k_wait_timeout_probe(int polls, int* status) {
-    __shared__ unsigned long long bar;
-    if (threadIdx.x == 0) {
-        mbar_init_one(&bar);
-        mbar_expect_tx(&bar, 16u);
-    }
-    __syncwarp();
-    const bool done = mbar_wait_bounded(&bar, 0, polls);
-    if (threadIdx.x == 0) *status = done ? 0 : MPM_ERR_COPY_TIMEOUT;
-}
-
-__device__ __forceinline__ void tma_load_box(void* dst, const CUtensorMap* map, int z0, int y0, int x0,
-                                             unsigned long long* bar) {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
-        "[%6];" ::"r"(smem_u32(dst)),
-        "l"(map), "r"(0), "r"(z0), "r"(y0), "r"(x0), "r"(smem_u32(bar))
-        : "memory");
-}
-
-// Box of base cells of the warp's lanes with an in-grid stencil, and the
-// TMA copy of its velocity nodes when it fits the fixed box (issued by lane
-// 0 as soon as the bases are known, so that it overlaps the particles' other
-// loads). Called by the whole warp.
-struct WarpBox {
-    int lo0, lo1, lo2;
-    int dims;   // ex | ey << 8 | ez << 16 | any << 24 | tma << 25 (extents <= 255 when used)
-    __device__ __forceinline__ int ex() const { return dims & 255; }
-    __device__ __forceinline__ int ey() const { return (dims >> 8) & 255; }
-    __device__ __forceinline__ int ez() const { return (dims >> 16) & 255; }
-    __device__ __forceinline__ bool any() const { return (dims >> 24) & 1; }
-    __device__ __forceinline__ bool tma() const { return (dims >> 25) & 1; }
-};
-
-// Computes the box and, when it fits, initialises the warp's mbarrier (one
-// use per launch) and issues the tensor copy (lane 0).
-__device__ __forceinline__ WarpBox warp_box_issue(const DevParams& P, const CUtensorMap* map, float4* vbox,
-                                                  unsigned long long* bar, bool part, const int base[3], int lane) {
-    WarpBox B;
-    B.lo0 = __reduce_min_sync(0xffffffffu, part ? base[0] : INT_MAX);
-    B.lo1 = __reduce_min_sync(0xffffffffu, part ? base[1] : INT_MAX);
-    B.lo2 = __reduce_min_sync(0xffffffffu, part ? base[2] : INT_MAX);
-    const int hi0 = __reduce_max_sync(0xffffffffu, part ? base[0] : INT_MIN);
-    const int hi1 = __reduce_max_sync(0xffffffffu, part ? base[1] : INT_MIN);
-    const int hi2 = __reduce_max_sync(0xffffffffu, part ? base[2] : INT_MIN);
-    const bool any = B.lo0 <= hi0;
-    const int ex = any ? hi0 - B.lo0 + 3 : 0, ey = any ? hi1 - B.lo1 + 3 : 0, ez = any ? hi2 - B.lo2 + 3 : 0;
-    const bool tma = any && ex <= kTmaBoxX && ey <= kTmaBoxY && ez <= kTmaBoxZ;
-    const bool small = any && ex <= 255 && ey <= 255 && ez <= 255;
-    B.dims = small ? (ex | (ey << 8) | (ez << 16) | (1 << 24) | ((int)tma << 25)) : 0;
-    if (tma && lane == 0) {
-        mbar_init_one(bar);
-        mbar_expect_tx(bar, kTmaBoxBytes);
-        tma_load_box(vbox, map, B.lo2, B.lo1, B.lo0 + P.halo, bar);
-    }
-    return B;
-}
-
-// Gather from the warp's box: the TMA copy issued by warp_box_issue when it
-// fit, else the warp's own coalesced loads (boxes up to VCAP nodes), else the
-// grid through L1. A copy that does not complete within the bounded wait
-// raises MPM_ERR_COPY_TIMEOUT, is waited for once more, and the warp gathers
-// through L1. Called by the whole warp.
-template <int VCAP>
-__device__ __forceinline__ void g2p_gather_tma(const DevParams& P, const WarpBox& B, const float4* __restrict__ vel,
-                                               float4* __restrict__ vbox, unsigned long long* bar, bool part,
-                                               bool active, const int base[3], const float fx[3], float v[3],
-                                               float C[3][3], int lane, WxSlot wx, int* err) {
-    const int lo0 = B.lo0, lo1 = B.lo1, lo2 = B.lo2;
-    int ey = B.ey(), ez = B.ez();
-    bool staged = false;
-    if (B.tma()) {
-        __syncwarp();
-        staged = mbar_wait_bounded(bar, 0);
-        if (!staged) {
-            if (lane == 0) raise_error(err, MPM_ERR_COPY_TIMEOUT);
-            mbar_wait_bounded(bar, 0);   // let the copy in flight land before the slice is left
-        }
-        ey = kTmaBoxY;
-        ez = kTmaBoxZ;
-    } else if (B.any() && B.ex() * ey * ez <= VCAP) {
-        const int vol = B.ex() * ey * ez;
-        const int slab = (int)P.slab, gz = P.Gz;
-        const int g0 = ((lo0 + P.halo) * P.Gy + lo1) * gz + lo2;
-        const float inv_ez = 1.0f / (float)ez, inv_ey = 1.0f / (float)ey;
-        for (int k = lane; k < vol; k += 32) {
-            const int row = (int)(((float)k + 0.5f) * inv_ez);   // k / ez (k, ez <= VCAP)
-            const int tz = k - row * ez;
-            const int tx = (int)(((float)row + 0.5f) * inv_ey);
-            const int ty = row - tx * ey;
-            vbox[k] = __ldg(vel + (g0 + tx * slab + ty * gz + tz));
-        }
-        __syncwarp();
-        staged = true;
-    }
-    if (part && staged) {
-        // v = sum w nv and the first moments M_k = sum w nv o_k over the node
-        // offsets o = (a, b, c); C = 4/h sum w nv (o - f) = 4/h (M - f v)
-        float ww[3][3];
-        quad_weights<float>(fx, ww);
-        wx.put(ww);
-        float Mx[3], My[3], Mz[3];
-#pragma unroll
-        for (int r = 0; r < 3; r++) { v[r] = 0.f; Mx[r] = 0.f; My[r] = 0.f; Mz[r] = 0.f; }
-        const int t0 = ((base[0] - lo0) * ey + (base[1] - lo1)) * ez + (base[2] - lo2);
-#pragma unroll 1
-        for (int a = 0; a < 3; a++) {
-            const float wa = wx.get(a);
-            float ra[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-            for (int b = 0; b < 3; b++) {
-                const float wab = wa * ww[b][1];
-                const float4* row = vbox + (t0 + a * ey * ez + b * ez);
-                float rb[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    const float4 nd = row[c];
-                    const float w = wab * ww[c][2];
-                    const float wn[3] = {w * nd.x, w * nd.y, w * nd.z};
-#pragma unroll
-                    for (int r = 0; r < 3; r++) {
-                        rb[r] += wn[r];
-                        if (c == 1) Mz[r] += wn[r];
-                        if (c == 2) Mz[r] += 2.0f * wn[r];
-                    }
-                }
-#pragma unroll
-                for (int r = 0; r < 3; r++) {
-                    ra[r] += rb[r];
-                    if (b == 1) My[r] += rb[r];
-                    if (b == 2) My[r] += 2.0f * rb[r];
-                }
-            }
-            const float fa = (float)a;
-#pragma unroll
-            for (int r = 0; r < 3; r++) {
-                v[r] += ra[r];
-                Mx[r] += fa * ra[r];
-            }
-        }
-        const float s4 = 4.0f * (float)P.h_inv;
-#pragma unroll
-        for (int r = 0; r < 3; r++) {
-            C[r][0] = s4 * (Mx[r] - fx[0] * v[r]);
-            C[r][1] = s4 * (My[r] - fx[1] * v[r]);
-            C[r][2] = s4 * (Mz[r] - fx[2] * v[r]);
-        }
-    } else if (active) {
-        g2p_gather_mixed(P, vel, base, fx, v, C, !part, wx);
-    }
-    __syncwarp();
-}
-
 // Return map of a crushed point in FP64 (mpm_kernels.cuh:486-544). Out of
 // line (it is rare and register-hungry); arguments and result travel by
 // value so that nothing of the caller is forced into local memory.
@@ -680,325 +482,6 @@ __device__ __forceinline__ void p2g_scatter_pairs(const DevParams& P, float4* __
             }
         }
     }
-}
-
-// One particle's stencil as a lane of the split scatter walks it: loop node
-// (a, b, c) is stencil node (a, b, c), or (2-a, 2-b, 2-c) when flipped. The
-// flip permutes the per-dimension weights already computed for the particle
-// (w_{2-k}(f) = w_k(2-f) for the quadratic B-spline), so each node gets the
-// same weight numbers as in the unsplit loop. The affine part is walked
-// incrementally: u = m v + S (x_node - x_p) at loop node (0,0,0), and each
-// loop step in a, b, c adds sh = +-h S[:,d] (minus when flipped).
-struct SplitStream {
-    float m, u[3], s0h[3], s1h[3], s2h[3], wa[2], wb[3], wc[3];
-};
-
-__device__ __forceinline__ void split_stream(const DevParams& P, SplitStream& H, float m, const float mv[3],
-                                             const float S[3][3], const float fx[3], bool flip) {
-    float ww[3][3];
-    quad_weights<float>(fx, ww);
-    const float h = (float)P.h;
-    const float sg = flip ? -h : h;
-    const float k0 = flip ? 2.0f : 0.0f;
-    H.m = m;
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        H.wb[k] = flip ? ww[2 - k][1] : ww[k][1];
-        H.wc[k] = flip ? ww[2 - k][2] : ww[k][2];
-        if (k < 2) H.wa[k] = flip ? ww[2 - k][0] : ww[k][0];
-    }
-    const float d0 = (k0 - fx[0]) * h, d1 = (k0 - fx[1]) * h, d2 = (k0 - fx[2]) * h;
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-        H.u[r] = mv[r] + S[r][0] * d0 + S[r][1] * d1 + S[r][2] * d2;
-        H.s0h[r] = S[r][0] * sg;
-        H.s1h[r] = S[r][1] * sg;
-        H.s2h[r] = S[r][2] * sg;
-    }
-}
-
-// Split scatter (SCATTER 5). Pairs as in p2g_scatter_pairs (two adjacent
-// lanes with the same base cell), but instead of shuffling 4 values per node
-// the pair exchanges its payloads once and each lane adds BOTH particles'
-// contributions over half of the 27 nodes: the first lane nodes 0..13 in
-// (a, b, c) order, the second the mirror images of its loop nodes 0..12,
-// i.e. nodes 26..14. A lone particle walks both halves itself, as two
-// streams: nodes 0..13, then the mirrored 26..14. Each lane runs 14 loop
-// nodes with two contributions each (27 of the 28 slots used) and one float4
-// atomic per node (pairs) or two (lone particles). Warps with a stencil
-// outside the grid take the checked loop of p2g_scatter_pairs.
-__device__ __forceinline__ void p2g_scatter_split(const DevParams& P, float4* __restrict__ acc, bool active,
-                                                  bool inside, const int base[3], const float fx[3], float mass,
-                                                  const float mv[3], const float S[3][3], int lane, WxSlot wx) {
-    if (!__all_sync(0xffffffffu, inside || !active)) {
-        p2g_scatter_pairs(P, acc, active, inside, base, fx, mass, mv, S, lane, wx);
-        return;
-    }
-    const int i0 = ((base[0] + P.halo) * P.Gy + base[1]) * P.Gz + base[2];
-    const int key = active ? i0 : -1 - lane;
-    const unsigned peers = __match_any_sync(0xffffffffu, key);
-    const int rank = __popc(peers & ((1u << lane) - 1u));
-    const int next_key = __shfl_down_sync(0xffffffffu, key, 1);
-    const bool first = lane < 31 && next_key == key && (rank & 1) == 0;
-    const bool second = __shfl_up_sync(0xffffffffu, (int)first, 1) != 0 && lane > 0;
-    const bool merged = first || second;
-    const int partner = first ? lane + 1 : (second ? lane - 1 : lane);
-    // the partner's payload (a lone lane reads its own)
-    float pm = __shfl_sync(0xffffffffu, mass, partner), pmv[3], pS[3][3], pfx[3];
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-        pmv[r] = __shfl_sync(0xffffffffu, mv[r], partner);
-        pfx[r] = __shfl_sync(0xffffffffu, fx[r], partner);
-#pragma unroll
-        for (int c = 0; c < 3; c++) pS[r][c] = __shfl_sync(0xffffffffu, S[r][c], partner);
-    }
-    // stream A: own particle, flipped on the second lane of a pair; stream B:
-    // the partner's particle on a pair's lanes (same flip), the own particle
-    // flipped on a lone lane (same base cell in every case)
-    SplitStream A, B;
-    split_stream(P, A, mass, mv, S, fx, second);
-    split_stream(P, B, pm, pmv, pS, pfx, !first);
-    const int slab = (int)P.slab, gz = P.Gz;
-    const int i0f = i0 + 2 * slab + 2 * gz + 2;   // loop node (0,0,0) of a flipped walk
-    const bool emit_a = active;
-    const bool emit_b = active && !merged;
-    // loop rows (a, b) = (0,0) (0,1) (0,2) (1,0) (1,1); u walks row starts
-#pragma unroll
-    for (int a = 0; a < 2; a++) {
-#pragma unroll
-        for (int b = 0; b < 3; b++) {
-            if (9 * a + 3 * b > 13) continue;
-            if (b > 0) {
-#pragma unroll
-                for (int r = 0; r < 3; r++) { A.u[r] += A.s1h[r]; B.u[r] += B.s1h[r]; }
-            } else if (a > 0) {
-#pragma unroll
-                for (int r = 0; r < 3; r++) {
-                    A.u[r] += A.s0h[r] - 2.0f * A.s1h[r];
-                    B.u[r] += B.s0h[r] - 2.0f * B.s1h[r];
-                }
-            }
-            const float wab_a = A.wa[a] * A.wb[b], wab_b = B.wa[a] * B.wb[b];
-            float za[3], zb[3];
-#pragma unroll
-            for (int r = 0; r < 3; r++) { za[r] = A.u[r]; zb[r] = B.u[r]; }
-            const int off_ab = a * slab + b * gz;
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const int j = 9 * a + 3 * b + c;
-                if (j > 13) continue;
-                if (c > 0) {
-#pragma unroll
-                    for (int r = 0; r < 3; r++) { za[r] += A.s2h[r]; zb[r] += B.s2h[r]; }
-                }
-                const float wa_ = wab_a * A.wc[c], wb_ = wab_b * B.wc[c];
-                float va[4] = {wa_ * A.m, wa_ * za[0], wa_ * za[1], wa_ * za[2]};
-                const float vb[4] = {wb_ * B.m, wb_ * zb[0], wb_ * zb[1], wb_ * zb[2]};
-                if (merged) {
-#pragma unroll
-                    for (int q = 0; q < 4; q++) va[q] += vb[q];
-                }
-                const int off = off_ab + c;
-                // the centre node (j == 13) belongs to the unflipped walk only
-                if (emit_a && !(j == 13 && second))
-                    atomicAdd(acc + (second ? i0f - off : i0 + off), make_float4(va[0], va[1], va[2], va[3]));
-                if (emit_b && j != 13)
-                    atomicAdd(acc + (first ? i0 + off : i0f - off), make_float4(vb[0], vb[1], vb[2], vb[3]));
-            }
-        }
-    }
-}
-
-// Shared-memory tile variant of the scatter. The block's particles (a
-// contiguous range of the cell-sorted order) span a small box of nodes; the
-// block accumulates the box with FP32 shared-memory atomics and adds each non-empty node to the grid once, as one
-// float4 vector atomic. Returns false (nothing done) when the box exceeds the
-// tile; the caller then scatters directly. Must be called by the whole block.
-template <int BLOCK>
-__device__ __forceinline__ bool p2g_scatter_tile(const DevParams& P, float4* __restrict__ acc, float* __restrict__ tile,
-                                                 int tile_cap, bool active, bool inside, const int base[3],
-                                                 const float fx[3], float mass, const float mv[3], const float S[3][3],
-                                                 int lane) {
-    __shared__ int s_box[6];
-    if (threadIdx.x < 3) { s_box[threadIdx.x] = INT_MAX; s_box[3 + threadIdx.x] = INT_MIN; }
-    __syncthreads();
-    const bool in_box = active && inside;
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-        int lo = in_box ? base[d] : INT_MAX, hi = in_box ? base[d] + 2 : INT_MIN;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-        }
-        if (lane == 0) { atomicMin(&s_box[d], lo); atomicMax(&s_box[3 + d], hi); }
-    }
-    __syncthreads();
-    const int bx = s_box[0], by = s_box[1], bz = s_box[2];
-    const int ex = s_box[3] - bx + 1, ey = s_box[4] - by + 1, ez = s_box[5] - bz + 1;
-    if (bx > s_box[3]) return true;   // no particle of the block is inside
-    const long long vol = (long long)ex * ey * ez;
-    if (vol > tile_cap) return false;
-    const int nv = (int)vol;
-    for (int k = threadIdx.x; k < 4 * nv; k += BLOCK) tile[k] = 0.f;
-    __syncthreads();
-    // particles of the block whose stencil leaves the grid go direct
-    if (active && !inside) {
-        p2g_scatter_mixed<false>(P, acc, active, inside, base, fx, mass, mv, S, lane);
-    } else {
-        const int t0 = ((base[0] - bx) * ey + (base[1] - by)) * ez + (base[2] - bz);
-        float ww[3][3];
-        quad_weights<float>(fx, ww);
-        const float h = (float)P.h;
-#pragma unroll 1
-        for (int a = 0; a < 3; a++) {
-            const float dx = (a - fx[0]) * h;
-#pragma unroll
-            for (int b = 0; b < 3; b++) {
-                const float dy = (b - fx[1]) * h;
-                const float wab = pick3(a, ww[0][0], ww[1][0], ww[2][0]) * ww[b][1];
-                const int tb = t0 + (a * ey + b) * ez;
-                float part[3];
-#pragma unroll
-                for (int m = 0; m < 3; m++) part[m] = mv[m] + S[m][0] * dx + S[m][1] * dy;
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    const float dz = (c - fx[2]) * h;
-                    const float W = wab * ww[c][2];
-                    if (!in_box) continue;
-                    const int t = tb + c;
-                    atomicAdd(tile + t, W * mass);
-                    atomicAdd(tile + nv + t, W * (part[0] + S[0][2] * dz));
-                    atomicAdd(tile + 2 * nv + t, W * (part[1] + S[1][2] * dz));
-                    atomicAdd(tile + 3 * nv + t, W * (part[2] + S[2][2] * dz));
-                }
-            }
-        }
-    }
-    __syncthreads();
-    const int slab = (int)P.slab, gz = P.Gz;
-    const int g0 = ((bx + P.halo) * P.Gy + by) * gz + bz;
-    for (int t = threadIdx.x; t < nv; t += BLOCK) {
-        const float m = tile[t];
-        if (m == 0.f) continue;
-        const int tz = t % ez, ty = (t / ez) % ey, tx = t / (ez * ey);
-        atomicAdd(acc + (g0 + tx * slab + ty * gz + tz), make_float4(m, tile[nv + t], tile[2 * nv + t], tile[3 * nv + t]));
-    }
-    return true;
-}
-
-// Shared-memory tile in 32-bit block fixed point. As p2g_scatter_tile, but
-// the tile holds integers: each contribution v is added as round(v * 2^e)
-// with native 32-bit shared atomics (order-independent sums), e chosen per
-// block from its largest possible contribution so that a node can absorb up
-// to 128 of them without overflow (2^-23 of that bound per unit). The flush
-// converts each node back to FP32 and adds it to the grid with one float4
-// atomic. Must be called by the whole block of 128 threads.
-__device__ __forceinline__ int fx32_exponent(float bound) {
-    int ex;
-    frexpf(fmaxf(bound, 1e-30f), &ex);   // bound < 2^ex
-    return 23 - ex;                        // 128 * bound * 2^e < 2^30
-}
-
-template <int BLOCK>
-__device__ __forceinline__ bool p2g_scatter_tile_fx(const DevParams& P, float4* __restrict__ acc, int* __restrict__ tile,
-                                                    int tile_cap, bool active, bool inside, const int base[3],
-                                                    const float fx[3], float mass, const float mv[3],
-                                                    const float S[3][3], int lane) {
-    __shared__ int s_box[8];
-    if (threadIdx.x < 3) { s_box[threadIdx.x] = INT_MAX; s_box[3 + threadIdx.x] = INT_MIN; }
-    if (threadIdx.x == 0) { s_box[6] = 0; s_box[7] = 0; }
-    __syncthreads();
-    const bool in_box = active && inside;
-    // bound of |w (m v + S (x_i - x_p))| over the stencil: w <= 1, |x_i - x_p| <= 1.5 h per axis
-    const float h15 = 1.5f * (float)P.h;
-    float pb = 0.f;
-    if (in_box) {
-#pragma unroll
-        for (int m = 0; m < 3; m++)
-            pb = fmaxf(pb, fabsf(mv[m]) + h15 * (fabsf(S[m][0]) + fabsf(S[m][1]) + fabsf(S[m][2])));
-    }
-    float mb = in_box ? mass : 0.f;
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-        int lo = in_box ? base[d] : INT_MAX, hi = in_box ? base[d] + 2 : INT_MIN;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-        }
-        if (lane == 0) { atomicMin(&s_box[d], lo); atomicMax(&s_box[3 + d], hi); }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        pb = fmaxf(pb, __shfl_xor_sync(0xffffffffu, pb, o));
-        mb = fmaxf(mb, __shfl_xor_sync(0xffffffffu, mb, o));
-    }
-    if (lane == 0) { atomicMax(&s_box[6], __float_as_int(pb)); atomicMax(&s_box[7], __float_as_int(mb)); }
-    __syncthreads();
-    const int bx = s_box[0], by = s_box[1], bz = s_box[2];
-    if (bx > s_box[3]) return true;   // no particle of the block is inside
-    const int ex = s_box[3] - bx + 1, ey = s_box[4] - by + 1, ez = s_box[5] - bz + 1;
-    const long long vol = (long long)ex * ey * ez;
-    if (vol > tile_cap) return false;
-    const int nv = (int)vol;
-    const int e_p = fx32_exponent(__int_as_float(s_box[6]));
-    const int e_m = fx32_exponent(__int_as_float(s_box[7]));
-    const float sc_p = ldexpf(1.0f, e_p), sc_m = ldexpf(1.0f, e_m);
-    for (int k = threadIdx.x; k < 4 * nv; k += BLOCK) tile[k] = 0;
-    __syncthreads();
-    if (active && !inside) {
-        p2g_scatter_mixed<false>(P, acc, active, inside, base, fx, mass, mv, S, lane);
-    } else if (in_box) {
-        const int t0 = ((base[0] - bx) * ey + (base[1] - by)) * ez + (base[2] - bz);
-        float ww[3][3];
-        quad_weights<float>(fx, ww);
-        const float h = (float)P.h;
-        const float msc = mass * sc_m;
-        float Ssc[3][3], mvsc[3];
-#pragma unroll
-        for (int m = 0; m < 3; m++) {
-            mvsc[m] = mv[m] * sc_p;
-#pragma unroll
-            for (int k = 0; k < 3; k++) Ssc[m][k] = S[m][k] * sc_p;
-        }
-#pragma unroll 1
-        for (int a = 0; a < 3; a++) {
-            const float dx = (a - fx[0]) * h;
-#pragma unroll
-            for (int b = 0; b < 3; b++) {
-                const float dy = (b - fx[1]) * h;
-                const float wab = pick3(a, ww[0][0], ww[1][0], ww[2][0]) * ww[b][1];
-                const int tb = t0 + (a * ey + b) * ez;
-                float part[3];
-#pragma unroll
-                for (int m = 0; m < 3; m++) part[m] = mvsc[m] + Ssc[m][0] * dx + Ssc[m][1] * dy;
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    const float dz = (c - fx[2]) * h;
-                    const float W = wab * ww[c][2];
-                    const int t = tb + c;
-                    atomicAdd(tile + t, __float2int_rn(W * msc));
-                    atomicAdd(tile + nv + t, __float2int_rn(W * (part[0] + Ssc[0][2] * dz)));
-                    atomicAdd(tile + 2 * nv + t, __float2int_rn(W * (part[1] + Ssc[1][2] * dz)));
-                    atomicAdd(tile + 3 * nv + t, __float2int_rn(W * (part[2] + Ssc[2][2] * dz)));
-                }
-            }
-        }
-    }
-    __syncthreads();
-    const float inv_m = ldexpf(1.0f, -e_m), inv_p = ldexpf(1.0f, -e_p);
-    const int slab = (int)P.slab, gz = P.Gz;
-    const int g0 = ((bx + P.halo) * P.Gy + by) * gz + bz;
-    for (int t = threadIdx.x; t < nv; t += BLOCK) {
-        const int m = tile[t];
-        if (m == 0) continue;
-        const int tz = t % ez, ty = (t / ez) % ey, tx = t / (ez * ey);
-        atomicAdd(acc + (g0 + tx * slab + ty * gz + tz),
-                  make_float4((float)m * inv_m, (float)tile[nv + t] * inv_p, (float)tile[2 * nv + t] * inv_p,
-                              (float)tile[3 * nv + t] * inv_p));
-    }
-    return true;
 }
 
 // P2G payload of a particle: S = m C - dt V Dp^-1 tau (mpm_kernels.cuh:63)
@@ -1193,24 +676,16 @@ __device__ __forceinline__ void fused_payload(const DevParams& P, bool active, c
 }
 
 // Fused G2P (this step) -> P2G (next step). do_p2g = 0 gives a plain G2P.
-// SCATTER: 0 = warp-reduced direct float4 atomics, 1 = direct float4
-// atomics, 2 = FP32 shared-memory tile, 3 = int32 fixed-point shared-memory
-// tile (2 and 3 fall back to 0 when the box is too big), 4 = direct float4
-// atomics with same-cell pairs merged, 5 = split scatter of merged pairs.
-// GATHER: 0 = from the grid through L1, 1 = from the warp's velocity box
-// staged in shared memory by the warp's loads (dynamic shared memory of
-// 4 x kVBoxNodes float4), 2 = the box brought in by one TMA tensor copy per
-// warp (4 x kTmaSliceNodes float4; vel_map).
+// 128-thread blocks at 8 per SM (64 registers). The gather reads the warp's
+// velocity box staged in shared memory by the warp's own coalesced loads
+// (4 x kVBoxNodes float4 of dynamic shared memory); the scatter adds float4
+// atomics with same-cell particle pairs merged in registers.
 constexpr int kVBoxNodes = 256;
-template <int MINB, int SCATTER, int GATHER = 0>
-__global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedState s, int n,
-                                                           const float4* __restrict__ vel, float4* __restrict__ acc,
-                                                           int do_p2g, int record_pq, int store_vc, int* err,
-                                                           int tile_cap, int* __restrict__ rm_list,
-                                                           int* __restrict__ rm_count,
-                                                           const __grid_constant__ CUtensorMap vel_map) {
+__global__ void __launch_bounds__(128, 8) k_g2p2g_mixed(DevParams P, MixedState s, int n,
+                                                        const float4* __restrict__ vel, float4* __restrict__ acc,
+                                                        int do_p2g, int record_pq, int store_vc, int* err,
+                                                        int* __restrict__ rm_list, int* __restrict__ rm_count) {
     extern __shared__ __align__(128) float mixed_tile[];
-    __shared__ unsigned long long vbox_bar[4];
     __shared__ float wx_slots[3 * 128];
     const WxSlot wx{wx_slots + threadIdx.x};
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1218,7 +693,7 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     bool active = i < n;
     int X[3] = {0, 0, 0}, st = (int)kDisabled;
     float E[3][3], Jpm1 = 0.f;
-    // positions and status first: the gather box (and its copy) depends on them
+    // positions and status first: the gather box depends on them
     if (active) {
         st = s.status[i];
 #pragma unroll
@@ -1237,10 +712,6 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
         e0 = stencil_error(P, base[0], base[1], base[2]);
         if (e0) raise_error(err, e0);
     }
-    float4* const vbox_tma = reinterpret_cast<float4*>(mixed_tile) + (threadIdx.x >> 5) * kTmaSliceNodes;
-    WarpBox wbox;
-    if (GATHER == 2)
-        wbox = warp_box_issue(P, &vel_map, vbox_tma, &vbox_bar[threadIdx.x >> 5], active && e0 == 0, base, lane);
     if (active) {
 #pragma unroll
         for (int r = 0; r < 3; r++)
@@ -1250,30 +721,15 @@ __global__ void __launch_bounds__(128, MINB) k_g2p2g_mixed(DevParams P, MixedSta
     }
     const int st_in = st;
     const float jpm1_in = Jpm1;
-    if (GATHER == 2) {
-        g2p_gather_tma<kTmaSliceNodes>(P, wbox, vel, vbox_tma, &vbox_bar[threadIdx.x >> 5], active && e0 == 0,
-                                       active, base, fx, v, C, lane, wx, err);
-    } else if (GATHER == 1) {
-        float4* vbox = reinterpret_cast<float4*>(mixed_tile) + (threadIdx.x >> 5) * kVBoxNodes;
-        g2p_gather_staged<kVBoxNodes>(P, vel, vbox, active && e0 == 0, active, base, fx, v, C, lane, wx);
-    } else if (active) {
-        g2p_gather_mixed(P, vel, base, fx, v, C, e0 != 0, wx);
-    }
+    float4* vbox = reinterpret_cast<float4*>(mixed_tile) + (threadIdx.x >> 5) * kVBoxNodes;
+    g2p_gather_staged<kVBoxNodes>(P, vel, vbox, active && e0 == 0, active, base, fx, v, C, lane, wx);
     const bool need_rm = fused_update_state(P, s, i, active, X, st, st_in, jpm1_in, E, Jpm1, v, C, inv, record_pq,
                                             store_vc, rm_list, rm_count, lane);
     active = active && !need_rm;   // crushed points scatter in k_return_map_mixed
     if (!do_p2g) return;   // uniform across the launch
     float mass, mv[3], S[3][3];
     fused_payload(P, active, X, st, E, C, v, Jpm1, inv, base, fx, mass, mv, S, inside, err);
-    if (SCATTER == 2 && p2g_scatter_tile<128>(P, acc, mixed_tile, tile_cap, active, inside, base, fx, mass, mv, S, lane))
-        return;
-    if (SCATTER == 3 && p2g_scatter_tile_fx<128>(P, acc, reinterpret_cast<int*>(mixed_tile), tile_cap, active, inside,
-                                                 base, fx, mass, mv, S, lane))
-        return;
-    if (SCATTER == 5) p2g_scatter_split(P, acc, active, inside, base, fx, mass, mv, S, lane, wx);
-    else if (SCATTER == 4) p2g_scatter_pairs(P, acc, active, inside, base, fx, mass, mv, S, lane, wx);
-    else if (SCATTER == 1) p2g_scatter_mixed<false>(P, acc, active, inside, base, fx, mass, mv, S, lane);
-    else p2g_scatter_mixed<true>(P, acc, active, inside, base, fx, mass, mv, S, lane);
+    p2g_scatter_pairs(P, acc, active, inside, base, fx, mass, mv, S, lane, wx);
 }
 
 // Return map (FP64, mpm_kernels.cuh:486-544) of the crushed points listed by

@@ -16,7 +16,6 @@
 #include <vector>
 
 #include <cuda.h>
-#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include "../../include/icempm_b200.h"
@@ -48,9 +47,6 @@ __global__ void k_iota(unsigned* __restrict__ ids, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) ids[i] = (unsigned)i;
 }
-constexpr int kMixedTileNodes = 2048;   // 32 KB FP32 tile of the fused mixed kernel
-constexpr int kFxBlock = 256;   // threads of the fixed-point P2G
-constexpr int kFxPPT = 4;       // particles per thread (1024-particle chunks)
 }  // namespace
 
 struct mpm_handle {
@@ -96,12 +92,7 @@ struct mpm_handle {
     float4* gacc = nullptr;
     float4* gvel = nullptr;
     bool p2g_ready = false;           // gacc holds the P2G of the current state
-    int mixed_variant = 3;            // fused kernel occupancy target: 3 = 8 blocks of 128 per SM (test hook)
-    int mixed_scatter = 4;            // fused kernel scatter: 0 warp-reduced, 1 direct, 2/3 tiles, 4 pairs (default)
-    int mixed_gather = 1;             // fused kernel gather: 0 through L1, 1 staged warp box (default)
     int num_sms = 148;
-    CUtensorMap vel_map;              // the velocity grid as a 4-D tensor for the TMA box copies
-    bool vel_map_ok = false;
     int* rm_list = nullptr;           // crushed points deferred to k_return_map_mixed (n entries)
     int* rm_counts = nullptr;         // two list counters, used alternately by successive launches
     int rm_parity = 0;
@@ -122,12 +113,6 @@ struct mpm_handle {
     std::vector<double*> adj_gcache;  // P2G grid of each substep of the segment being reversed
     double* adj_rmv = nullptr;        // return-map VJP of the crushed points (10 x pitch)
 
-    int p2g_variant = 5;              // see mpm_testing_set_p2g_variant (5: pair-merged, 6 per SM)
-    int g2p_variant = 0;              // see mpm_testing_set_g2p_variant (0: 4 blocks of 128 per SM)
-    int tile_cap = 2048;              // P2G tile nodes (x 32 B of shared memory)
-    int fx_tile_cap = 3072;           // nodes of the fixed-point tile (x 32 B)
-    float* chunk_bound = nullptr;     // per-chunk |contribution| bound of the fixed-point P2G
-    int chunk_bound_cap = 0;
 
     // animation-frame records (mpm_frame_records), allocated on first use
     float* fr_f = nullptr;            // visual state: pos 3, vel 3, Jp_inv rows x pitch
@@ -224,7 +209,6 @@ void free_all(mpm_handle* h) {
     cudaFree(h->force_steps); cudaFree(h->force_phase); cudaFree(h->err);
     cudaFree(h->pts_alt); cudaFree(h->p0_alt); cudaFree(h->ids_alt);
     cudaFree(h->s_bucket); cudaFree(h->s_count); cudaFree(h->s_start); cudaFree(h->s_perm);
-    cudaFree(h->chunk_bound);
     cudaFree(h->mx); cudaFree(h->p0f); cudaFree(h->gacc); cudaFree(h->gvel);
     cudaFree(h->rm_list); cudaFree(h->rm_counts);
     for (double* c : h->ckpt) cudaFree(c);
@@ -297,42 +281,7 @@ int launch_p2g(mpm_handle* h) {
         CK_LAUNCH(h, "p2g mixed");
         return MPM_OK;
     }
-    const size_t smem = sizeof(double) * 4 * h->tile_cap;
-    switch (h->p2g_variant) {
-        case 1:
-            k_p2g_direct_f64<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, h->err);
-            break;
-        case 2:
-            k_p2g_warpagg_f64<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, h->err);
-            break;
-        case 5:
-            k_p2g_pairs_f64<6><<<blocks_for(n, 128), 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, h->err);
-            break;
-        case 6:
-            k_p2g_pairs_f64<4><<<blocks_for(n, 128), 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, h->err);
-            break;
-        case 3:
-            k_p2g_tile_f64<256, true><<<blocks_for(n, 256), 256, smem, h->stream>>>(h->dp, h->pts, h->pitch, n,
-                                                                                     h->grid, h->err, h->tile_cap);
-            break;
-        case 4: {
-            const int chunks = (int)blocks_for(n, kFxBlock * kFxPPT);
-            if (chunks > h->chunk_bound_cap) {
-                cudaFree(h->chunk_bound);
-                h->chunk_bound = nullptr;
-                CK(h, cudaMalloc(&h->chunk_bound, sizeof(float) * chunks));
-                CK(h, cudaMemsetAsync(h->chunk_bound, 0, sizeof(float) * chunks, h->stream));
-                h->chunk_bound_cap = chunks;
-            }
-            k_p2g_fx_f64<kFxBlock, kFxPPT><<<chunks, kFxBlock, sizeof(long long) * 4 * h->fx_tile_cap, h->stream>>>(
-                h->dp, h->pts, h->pitch, n, h->grid, h->err, h->fx_tile_cap, h->chunk_bound);
-            break;
-        }
-        default:
-            k_p2g_tile_f64<256, false><<<blocks_for(n, 256), 256, smem, h->stream>>>(h->dp, h->pts, h->pitch, n,
-                                                                                      h->grid, h->err, h->tile_cap);
-            break;
-    }
+    k_p2g_pairs_f64<<<blocks_for(n, 128), 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, h->err);
     CK_LAUNCH(h, "p2g kernel");
     return MPM_OK;
 }
@@ -348,36 +297,6 @@ int launch_update(mpm_handle* h, double ind_x, double ind_y, double* force3) {
                                                                              force3);
     CK_LAUNCH(h, "update kernel");
     return MPM_OK;
-}
-
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
-// against libcuda); null when the driver does not provide it.
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    });
-    return fn;
-}
-
-// The float4 velocity grid as the 4-D FP32 tensor (component, z, y, x) with
-// the fixed gather box of the TMA path: 4 x kTmaBoxZ x kTmaBoxY x kTmaBoxX.
-bool make_vel_map(mpm_handle* h) {
-    auto enc = tensor_map_encoder();
-    if (!enc) return false;
-    const DevParams& d = h->dp;
-    const cuuint64_t dims[4] = {4, (cuuint64_t)d.Gz, (cuuint64_t)d.Gy, (cuuint64_t)(d.nodes / d.slab)};
-    const cuuint64_t strides[3] = {16, 16ull * (cuuint64_t)d.Gz, 16ull * (cuuint64_t)d.slab};
-    const cuuint32_t box[4] = {4, (cuuint32_t)kTmaBoxZ, (cuuint32_t)kTmaBoxY, (cuuint32_t)kTmaBoxX};
-    const cuuint32_t estr[4] = {1, 1, 1, 1};
-    return enc(&h->vel_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->gvel, dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // Return map and P2G of the crushed points the last fused launch listed
@@ -398,63 +317,11 @@ int launch_return_map_mixed(mpm_handle* h, int do_p2g) {
 int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
     const int n = (int)h->n;
     if (n == 0) return MPM_OK;
-    const unsigned nb = blocks_for(n, 128);
-    const int sc = h->mixed_scatter;
     int* const rm_count = h->rm_counts + h->rm_parity;
-    if (h->mixed_gather == 2 && h->vel_map_ok) {
-        // TMA gather box: 4 warps x kTmaSliceNodes float4 of dynamic shared memory
-        const size_t tmsm = sizeof(float4) * 4 * kTmaSliceNodes;
-        if (sc >= 4)   // the pair-merged scatters (9, 10) run as 9 here
-            k_g2p2g_mixed<8, 4, 2><<<nb, 128, tmsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,
-                                                                 record_pq, store_vc, h->err, 0, h->rm_list, rm_count,
-                                                                 h->vel_map);
-        else
-            k_g2p2g_mixed<8, 1, 2><<<nb, 128, tmsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,
-                                                                 record_pq, store_vc, h->err, 0, h->rm_list, rm_count,
-                                                                 h->vel_map);
-        CK_LAUNCH(h, "g2p2g mixed (TMA gather)");
-        return MPM_OK;
-    }
-    if (h->mixed_gather) {
-        // staged gather: 4 warps x kVBoxNodes float4 of dynamic shared memory
-        const size_t vsm = sizeof(float4) * 4 * kVBoxNodes;
-#define FUSED_G(MINB, SC)                                                                                           \
-    k_g2p2g_mixed<MINB, SC, 1><<<nb, 128, vsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,    \
-                                                            record_pq, store_vc, h->err, 0, h->rm_list, rm_count,  \
-                                                            h->vel_map)
-        if (h->mixed_variant == 1) {
-            if (sc >= 4) FUSED_G(5, 4);
-            else if (sc == 0) FUSED_G(5, 0);
-            else FUSED_G(5, 1);
-        } else if (h->mixed_variant == 3) {
-            if (sc == 5) FUSED_G(8, 5);
-            else if (sc == 4) FUSED_G(8, 4);
-            else FUSED_G(8, 1);
-        } else {
-            if (sc >= 4) FUSED_G(6, 4);
-            else if (sc == 0) FUSED_G(6, 0);
-            else FUSED_G(6, 1);
-        }
-#undef FUSED_G
-        CK_LAUNCH(h, "g2p2g mixed (staged gather)");
-        return MPM_OK;
-    }
-    const size_t tsm = (sc == 2 || sc == 3) ? sizeof(float) * 4 * kMixedTileNodes : 0;
-#define FUSED(MINB, SC)                                                                                          \
-    k_g2p2g_mixed<MINB, SC><<<nb, 128, tsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,     \
-                                                         record_pq, store_vc, h->err, kMixedTileNodes, h->rm_list,  \
-                                                         rm_count, h->vel_map)
-#define FUSED_SC(MINB)                  \
-    if (sc >= 4) FUSED(MINB, 4);        \
-    else if (sc == 3) FUSED(MINB, 3);   \
-    else if (sc == 2) FUSED(MINB, 2);   \
-    else if (sc == 1) FUSED(MINB, 1);   \
-    else FUSED(MINB, 0);
-    if (h->mixed_variant == 1) { FUSED_SC(5) }
-    else if (h->mixed_variant == 2) { FUSED_SC(6) }
-    else { FUSED_SC(4) }
-#undef FUSED_SC
-#undef FUSED
+    // the warps' velocity boxes: 4 warps x kVBoxNodes float4 of dynamic shared memory
+    const size_t vsm = sizeof(float4) * 4 * kVBoxNodes;
+    k_g2p2g_mixed<<<blocks_for(n, 128), 128, vsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,
+                                                              record_pq, store_vc, h->err, h->rm_list, rm_count);
     CK_LAUNCH(h, "g2p2g mixed");
     return MPM_OK;
 }
@@ -467,20 +334,10 @@ int launch_g2p(mpm_handle* h, int record_pq) {
         return r ? r : launch_return_map_mixed(h, 0);
     }
     const unsigned nb = blocks_for(n, 128);
-    const bool f32svd = h->precision == MPM_PRECISION_FP64;
-#define G2P_LAUNCH(MINB)                                                                                        \
-    if (f32svd)                                                                                                 \
-        k_g2p_f64<SvdF32, MINB><<<nb, 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, record_pq, h->p0, \
-                                                           h->err);                                             \
-    else                                                                                                        \
-        k_g2p_f64<SvdF64, MINB><<<nb, 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, record_pq, h->p0, \
-                                                           h->err);
-    switch (h->g2p_variant) {
-        case 1: G2P_LAUNCH(3) break;
-        case 2: G2P_LAUNCH(6) break;
-        default: G2P_LAUNCH(4) break;
-    }
-#undef G2P_LAUNCH
+    if (h->precision == MPM_PRECISION_FP64)
+        k_g2p_f64<SvdF32><<<nb, 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, record_pq, h->p0, h->err);
+    else
+        k_g2p_f64<SvdF64><<<nb, 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, record_pq, h->p0, h->err);
     CK_LAUNCH(h, "g2p kernel");
     return MPM_OK;
 }
@@ -656,15 +513,6 @@ mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity
         if (cudaSetDevice(device) != cudaSuccess) { st = MPM_ERR_CUDA; break; }
         if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) { st = MPM_ERR_CUDA; break; }
         h->stream = h->own_stream;
-        if (cudaFuncSetAttribute(k_p2g_tile_f64<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(sizeof(double) * 4 * h->tile_cap)) != cudaSuccess ||
-            cudaFuncSetAttribute(k_p2g_tile_f64<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(sizeof(double) * 4 * h->tile_cap)) != cudaSuccess ||
-            cudaFuncSetAttribute(k_p2g_fx_f64<kFxBlock, kFxPPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(sizeof(long long) * 4 * h->fx_tile_cap)) != cudaSuccess) {
-            st = MPM_ERR_CUDA;
-            break;
-        }
         const size_t ns = sensor_count(*prms);
         if (cudaMalloc(&h->pts, sizeof(double) * MPM_N_PTS_ARRAYS * h->pitch) != cudaSuccess ||
             cudaMalloc(&h->ids, sizeof(unsigned) * h->pitch) != cudaSuccess ||
@@ -685,8 +533,6 @@ mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity
                 break;
             }
             cudaMemsetAsync(h->rm_counts, 0, sizeof(int) * 2, h->stream);
-            std::memset(&h->vel_map, 0, sizeof(h->vel_map));
-            h->vel_map_ok = make_vel_map(h);
             cudaMemsetAsync(h->mx, 0, sizeof(float) * MPM_N_PTS_ARRAYS * h->pitch, h->stream);
             cudaMemsetAsync(h->gacc, 0, sizeof(float4) * (size_t)h->dp.nodes, h->stream);
             cudaMemsetAsync(h->gvel, 0, sizeof(float4) * (size_t)h->dp.nodes, h->stream);
@@ -1180,19 +1026,6 @@ int mpm_testing_step_timed(mpm_handle* h, int nsteps, float* ms) {
     return r;
 }
 
-int mpm_testing_copy_wait_timeout(int device, int polls, int* status) {
-    if (!status || polls <= 0) return MPM_ERR_ARG;
-    if (cudaSetDevice(device) != cudaSuccess) return MPM_ERR_NO_DEVICE;
-    int* d = nullptr;
-    if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return MPM_ERR_CUDA;
-    cudaMemset(d, 0xff, sizeof(int));
-    k_wait_timeout_probe<<<1, 32>>>(polls, d);
-    cudaError_t e = cudaDeviceSynchronize();
-    if (e == cudaSuccess) e = cudaMemcpy(status, d, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaFree(d);
-    return e == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
-}
-
 int mpm_testing_active_nodes(mpm_handle* h, long long* count) {
     if (!h || !count) return MPM_ERR_ARG;
     const size_t nodes = (size_t)h->dp.nodes;
@@ -1209,21 +1042,6 @@ int mpm_testing_active_nodes(mpm_handle* h, long long* count) {
         for (size_t i = 0; i < nodes; i++) c += m[i] != 0.0;
     }
     *count = c;
-    return MPM_OK;
-}
-
-int mpm_testing_set_g2p_variant(mpm_handle* h, int variant) {
-    if (!h || variant < 0 || variant > 6) return MPM_ERR_ARG;
-    if (variant >= 3) {
-        if (!is_mixed(h)) return MPM_ERR_ARG;
-        if (variant == 6 && !h->vel_map_ok) return MPM_ERR_ARG;
-        h->mixed_variant = variant == 3 ? 2 : variant == 4 ? 1 : 3;
-        h->mixed_gather = variant == 6 ? 2 : 1;
-        return MPM_OK;
-    }
-    h->g2p_variant = variant;
-    h->mixed_variant = variant;
-    h->mixed_gather = 0;
     return MPM_OK;
 }
 
@@ -1247,18 +1065,6 @@ int mpm_testing_download_grid(mpm_handle* h, double* out, int which) {
         CK(h, cudaMemcpyAsync(out + c * nodes, h->grid + c * h->dp.gstride, sizeof(double) * nodes,
                               cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
-    return MPM_OK;
-}
-
-int mpm_testing_set_p2g_variant(mpm_handle* h, int variant) {
-    if (!h || variant < 0 || variant > 10) return MPM_ERR_ARG;
-    if (is_mixed(h)) {
-        if (variant < 5) return MPM_ERR_ARG;
-        h->mixed_scatter = variant - 5;
-        return MPM_OK;
-    }
-    if (variant > 6) return MPM_ERR_ARG;
-    h->p2g_variant = variant;
     return MPM_OK;
 }
 

@@ -30,7 +30,6 @@ ERR_NAMES = {
     104: "configuration file not found", 105: "configuration file is not JSON / wrong key type",
     106: "config parameter missing (InputRawPoints)", 107: "cell key outside the grid",
     108: "call out of order", 109: "size beyond the fixed scratch of the allocation-free sort",
-    110: "a bounded wait on an asynchronous copy in a kernel ran out",
 }
 
 

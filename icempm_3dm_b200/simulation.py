@@ -172,12 +172,6 @@ class MPMHandle:
         check(LIB.mpm_testing_active_nodes(self._h, ctypes.byref(c)), "mpm_testing_active_nodes")
         return c.value
 
-    def set_g2p_variant(self, v):
-        check(LIB.mpm_testing_set_g2p_variant(self._h, v), "mpm_testing_set_g2p_variant")
-
-    def set_p2g_variant(self, v):
-        check(LIB.mpm_testing_set_p2g_variant(self._h, v), "mpm_testing_set_p2g_variant")
-
     # -- adjoint (FP64 handles)
     def adjoint_forward(self, nsteps, ckpt_every):
         """nsteps substeps with a device checkpoint every ckpt_every; returns

@@ -46,7 +46,6 @@ extern "C" {
 #define MPM_ERR_SORT_RANGE   107  /* a particle's cell key lies outside grid */
 #define MPM_ERR_STATE        108  /* call out of order (e.g. step before upload) */
 #define MPM_ERR_NOALLOC_LIMIT 109 /* size beyond the fixed scratch of mpm_sort_permutation_noalloc */
-#define MPM_ERR_COPY_TIMEOUT 110  /* a bounded wait on an asynchronous (TMA) copy in a kernel ran out */
 
 #define MPM_PRECISION_FP64   0    /* FP64 state and transfers; 3x3 SVD in FP32
                                      exactly as the reference (helper_math.cuh) */

@@ -3,7 +3,7 @@
   block250k  FP64 GPU vs the CPU oracle (reference semantics, FP32 SVD),
              1,000 substeps: indenter force per substep and final state.
   block2m    FP64 at scale with lognormal per-particle cohesion, GPU vs the
-             oracle over 400 substeps.
+             oracle over the configuration's 2,000 substeps.
   block8m    mixed vs FP64 (FP64 SVD) on the GPU, 2,000 substeps: force
              history within 1e-3 relative (the required bound) and the error
              of each output field, printed.
@@ -12,7 +12,7 @@
              particle copy and on the full 500,000-particle block (plus its 8
              largest gradients); adjoint vs the FP64 dual-number forward
              mode on the 20,000-particle copy over 200 substeps.
-  grains30m  the non-uniform 30 M case, 1,000 substeps: mixed vs FP64 force
+  grains30m  the non-uniform 30 M case, 5,000 substeps: mixed vs FP64 force
              history within 1e-3 and the error of each output field, printed;
              size-independent properties (sorted cell keys, finite state).
 """
@@ -93,13 +93,15 @@ def test_block250k_fp64_matches_oracle_over_1000_substeps():
     print("\nblock250k FP64 vs oracle: " + "; ".join(lines))
 
 
-def test_block2m_fp64_with_lognormal_cohesion_matches_oracle():
+def test_block2m_fp64_with_lognormal_cohesion_matches_oracle_over_2000_substeps():
     """The FP64-at-scale workload (2,000,000 particles, h 0.0125 m, lognormal
     per-particle cohesion, indenter at 0.5 m/s) on the GPU against the oracle
     on the host cores, with the same apex shift p0 = c / tan(phi) per particle
-    (the device forms it with the same correctly rounded division). 400
-    substeps: the span in which rounding differences of the FP64 atomics'
-    order have not yet met a discrete switch (block250k above)."""
+    (the device forms it with the same correctly rounded division), over the
+    configuration's 2,000 substeps. As for block250k: tight agreement while
+    the FP64 atomics' rounding has met no discrete switch (400 substeps), and
+    at 2,000 a GPU-oracle distance within 5x the GPU's own run-to-run spread
+    (floor 1e-3 in force, 1e-6 m in position)."""
     prms, soa, coh = gen.make_block(gen.CONFIGS["block2m"])
     n = soa.shape[1]
     perm = po.sort_permutation(prms, soa, n)
@@ -107,16 +109,21 @@ def test_block2m_fp64_with_lognormal_cohesion_matches_oracle():
     coh = np.ascontiguousarray(coh[perm])
     assert coh.std() > 0.2 * coh.mean()   # non-uniform strength
     p0 = coh / prms.DP_tan_phi
-    marks = (200, 400)
-    hist, outs = [], []
-    with MPMHandle(prms, n, PRECISION_FP64) as h:
-        h.upload(soa, cohesion=coh)
-        done = 0
-        for m in marks:
-            hist.append(h.step(m - done))
-            done = m
-            outs.append(h.download())
-    hist = np.concatenate(hist)
+    marks = (400, 2000)
+
+    def gpu_run():
+        hist, outs = [], []
+        with MPMHandle(prms, n, PRECISION_FP64) as h:
+            h.upload(soa, cohesion=coh)
+            done = 0
+            for m in marks:
+                hist.append(h.step(m - done))
+                done = m
+                outs.append(h.download())
+        return np.concatenate(hist), outs
+
+    g1, o1 = gpu_run()
+    g2, o2 = gpu_run()
     sim = po.OracleSim(prms, soa, n, p0=p0, svd_mode=0, nthreads=os.cpu_count() or 1)
     ref_hist, ref_out, done = [], [], 0
     for m in marks:
@@ -129,14 +136,21 @@ def test_block2m_fp64_with_lognormal_cohesion_matches_oracle():
     assert np.linalg.norm(ref_hist[:, 0]) > 0
     lines = []
     for k, m in enumerate(marks):
-        e = rel(hist[:m], ref_hist[:m])
-        x = float(np.abs(outs[k][POSX:POSX + 3] - ref_out[k][POSX:POSX + 3]).max())
-        f = rel(outs[k][FE00:FE00 + 9], ref_out[k][FE00:FE00 + 9])
-        flips = int(np.sum(crushed(outs[k]) != crushed(ref_out[k])))
-        lines.append(f"{m} substeps: force {e:.2e}, positions {x:.2e} m, F {f:.2e}, "
-                     f"crushed {int(crushed(outs[k]).sum())}, flag differences {flips}")
-        assert e < 1e-7 and x < 1e-10 and f < 1e-9
+        e = rel(g1[:m], ref_hist[:m])
+        e_run = rel(g1[:m], g2[:m])
+        x = float(np.abs(o1[k][POSX:POSX + 3] - ref_out[k][POSX:POSX + 3]).max())
+        x_run = float(np.abs(o1[k][POSX:POSX + 3] - o2[k][POSX:POSX + 3]).max())
+        f = rel(o1[k][FE00:FE00 + 9], ref_out[k][FE00:FE00 + 9])
+        flips = int(np.sum(crushed(o1[k]) != crushed(ref_out[k])))
+        lines.append(f"{m} substeps: force {e:.2e} (GPU run to run {e_run:.2e}), positions {x:.2e} m "
+                     f"(run to run {x_run:.2e} m), F {f:.2e}, crushed {int(crushed(o1[k]).sum())}, "
+                     f"flag differences {flips}")
         assert flips <= n * 1e-5
+        if m == 400:
+            assert e < 1e-7 and x < 1e-10 and f < 1e-9
+        else:
+            assert e <= max(5 * e_run, 1e-3)
+            assert x <= max(5 * x_run, 1e-6)
     print("\nblock2m FP64 vs oracle: " + "; ".join(lines))
 
 
@@ -289,15 +303,16 @@ def grains():
 
 
 def test_grains30m_mixed_vs_fp64_and_sorted_keys(grains):
-    """Both precisions on the 30 M-particle non-uniform case, 1,000 substeps
-    (a fifth of the configuration's 5,000): the force history within 1e-3,
+    """Both precisions on the 30 M-particle non-uniform case over the
+    configuration's 5,000 substeps: the force history within 1e-3,
     the error of each output field printed, and the cell keys non-decreasing
     after the sort. Fields are compared in particle-id order, one block of
     rows at a time."""
     import psutil
     prms, soa, coh = grains
     n = soa.shape[1]
-    steps = 1000
+    steps = gen.CONFIGS["grains30m"].steps
+    assert steps == 5000
     # two full downloads of 28 rows x 30 M doubles (6.7 GB each) are held for
     # the field comparison; with less free host memory only the force history
     # is compared

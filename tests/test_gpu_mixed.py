@@ -34,18 +34,11 @@ def test_upload_download_round_trip():
     assert np.array_equal(util_bits(out), util_bits(soa))
 
 
-# (p2g/scatter variant, g2p/gather variant) pairs of the fused kernel
-FUSED_VARIANTS = [(5, 2), (6, 2), (7, 2), (8, 2), (9, 2), (6, 3), (9, 3), (9, 4), (9, 5), (9, 6), (6, 6), (10, 5)]
-
-
-@pytest.mark.parametrize("scatter,gather", FUSED_VARIANTS)
-def test_single_step_phases_close_to_oracle(scatter, gather):
+def test_single_step_phases_close_to_oracle():
     prms, soa = perturbed_block(n=4000, seed=31)
     n = soa.shape[1]
     ix = prms.indenter_x + 0.02
     with MPMHandle(prms, n, PRECISION_MIXED) as h:
-        h.set_p2g_variant(scatter)
-        h.set_g2p_variant(gather)
         h.upload(soa)
         h.reset_indenter_force_accumulator()
         h.reset_grid()
@@ -78,14 +71,11 @@ def test_single_step_phases_close_to_oracle(scatter, gather):
     assert rel_dev(out[IDX_JP_INV][same], ref[IDX_JP_INV][same]) < 1e-5
 
 
-@pytest.mark.parametrize("scatter,gather", FUSED_VARIANTS)
-def test_force_history_within_1e3_of_fp64(scatter, gather):
+def test_force_history_within_1e3_of_fp64():
     prms, soa = perturbed_block(n=3000, seed=41, ind_velocity=0.5, crushed_frac=0.05, strong_frac=0.0)
     n = soa.shape[1]
     steps = 60
     with MPMHandle(prms, n, PRECISION_MIXED) as h:
-        h.set_p2g_variant(scatter)
-        h.set_g2p_variant(gather)
         h.upload(soa)
         hist = h.step(steps)
         out = h.download()
@@ -144,8 +134,7 @@ def test_split_calls_and_periodic_sort_keep_state():
     assert np.abs(f1[VELX:VELX + 3] - f2[VELX:VELX + 3]).max() < 1e-4 * np.abs(f1[VELX:VELX + 3]).max()
 
 
-@pytest.mark.parametrize("scatter,gather", [(9, 5), (6, 2)])
-def test_liquid_and_disabled_particles_in_the_fused_path(scatter, gather):
+def test_liquid_and_disabled_particles_in_the_fused_path():
     """Water points (status 0x40000: Kirchhoff stress replaced by the water
     pressure, Jp_inv advected by det(I + dt C)) and disabled points (skipped)
     through the mixed fused kernel, against the FP64-SVD oracle."""
@@ -167,8 +156,6 @@ def test_liquid_and_disabled_particles_in_the_fused_path(scatter, gather):
     soa[IDX_UTILITY] = util_as_double(bits)
     steps = 30
     with MPMHandle(prms, n, PRECISION_MIXED) as h:
-        h.set_p2g_variant(scatter)
-        h.set_g2p_variant(gather)
         h.upload(soa)
         held = h.download()         # the state as the mixed handle holds it (FP32 rounding)
         hist = h.step(steps)
