@@ -31,6 +31,11 @@ struct DevParams {
     double drag;
     // failure-surface constants for GrainVariability = 0 (FP32 fast path)
     float fs_pmin2, fs_k, fs_msq, fs_1p2b, fs_bpmax, fs_pmax;
+    // FP32 copies for the mixed kernels, rounded once on the host (constant-
+    // bank operands there, instead of a double multiply and a conversion in
+    // every thread): h, 1/h, 4/h, dt, dt/h 2^20 (fixed-point advection), mu,
+    // kappa, kappa/2, sqrt(3/2) mu, particle and liquid mass, dt V Dp^-1
+    float f_h, f_h_inv, f_s4, f_dt, f_adv, f_mu, f_kappa, f_hkappa, f_qmu, f_pmass, f_lmass, f_dvd;
     double inv_gz, inv_gy;         // 1 / Gz, 1 / Gy for node index -> (x, y, z)
 };
 

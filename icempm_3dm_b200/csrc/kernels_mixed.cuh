@@ -91,18 +91,18 @@ __device__ __forceinline__ ElasticInv elastic_invariants(const float E[3][3]) {
 }
 
 __device__ __forceinline__ void trial_pq_inv(const DevParams& P, const ElasticInv& e, float& p_tr, float& q_tr) {
-    p_tr = -(float)(0.5 * P.kappa) * (e.jm1 * (e.J + 1.0f));
+    p_tr = -P.f_hkappa * (e.jm1 * (e.J + 1.0f));
     float sq = 0.f;
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
         for (int j = 0; j < 3; j++) sq += e.D[i][j] * e.D[i][j];
-    q_tr = (float)(kCoeff1 * P.mu) * e.jm23 * sqrtf(sq);
+    q_tr = P.f_qmu * e.jm23 * sqrtf(sq);
 }
 
 __device__ __forceinline__ void tau_inv(const DevParams& P, const ElasticInv& e, float tau[3][3]) {
-    const float s = (float)P.mu * e.jm23;
-    const float hyd = (float)(P.kappa * 0.5) * (e.jm1 * (e.J + 1.0f));
+    const float s = P.f_mu * e.jm23;
+    const float hyd = P.f_hkappa * (e.jm1 * (e.J + 1.0f));
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -127,8 +127,8 @@ __device__ __forceinline__ void kirchhoff_mixed(const DevParams& P, const float 
     const float J = 1.0f + jm1;
     float D[3][3];
     dev_b(E, D);
-    const float s = (float)P.mu * exp2f(-(2.0f / 3.0f) * log2f(J));
-    const float hyd = (float)(P.kappa * 0.5) * (jm1 * (J + 1.0f));
+    const float s = P.f_mu * exp2f(-(2.0f / 3.0f) * log2f(J));
+    const float hyd = P.f_hkappa * (jm1 * (J + 1.0f));
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -140,7 +140,7 @@ __device__ __forceinline__ void trial_pq_mixed(const DevParams& P, const float E
                                                float& q_tr) {
     jm1 = detm1(E);
     const float J = 1.0f + jm1;
-    p_tr = -(float)(0.5 * P.kappa) * (jm1 * (J + 1.0f));
+    p_tr = -P.f_hkappa * (jm1 * (J + 1.0f));
     float D[3][3];
     dev_b(E, D);
     float sq = 0.f;
@@ -148,7 +148,7 @@ __device__ __forceinline__ void trial_pq_mixed(const DevParams& P, const float E
     for (int i = 0; i < 3; i++)
 #pragma unroll
         for (int j = 0; j < 3; j++) sq += D[i][j] * D[i][j];
-    q_tr = (float)(kCoeff1 * P.mu) * exp2f(-(2.0f / 3.0f) * log2f(J)) * sqrtf(sq);
+    q_tr = P.f_qmu * exp2f(-(2.0f / 3.0f) * log2f(J)) * sqrtf(sq);
 }
 
 // w[a] of a 3-entry weight column with a loop counter that is not unrolled:
@@ -188,7 +188,7 @@ __device__ __forceinline__ void g2p_gather_mixed(const DevParams& P, const float
 #pragma unroll
         for (int k = 0; k < 3; k++) C[d][k] = 0.f;
     }
-    const float s4 = 4.0f * (float)P.h_inv;
+    const float s4 = P.f_s4;
     const int slab = (int)P.slab, gz = P.Gz;
     const int i0 = ((base[0] + P.halo) * P.Gy + base[1]) * gz + base[2];
 #pragma unroll 1
@@ -306,7 +306,7 @@ __device__ __forceinline__ void g2p_gather_staged(const DevParams& P, const floa
                 Mx[r] += fa * ra[r];
             }
         }
-        const float s4 = 4.0f * (float)P.h_inv;
+        const float s4 = P.f_s4;
 #pragma unroll
         for (int r = 0; r < 3; r++) {
             C[r][0] = s4 * (Mx[r] - fx[0] * v[r]);
@@ -361,7 +361,7 @@ __device__ __forceinline__ void p2g_scatter_mixed(const DevParams& P, float4* __
     const int rounds = AGG ? (int)__reduce_max_sync(0xffffffffu, (unsigned)(__popc(peers) - 1)) : 0;
     float ww[3][3];
     quad_weights<float>(fx, ww);
-    const float h = (float)P.h;
+    const float h = P.f_h;
     const int slab = (int)P.slab, gz = P.Gz;
 #pragma unroll 1
     for (int a = 0; a < 3; a++) {
@@ -420,7 +420,7 @@ __device__ __forceinline__ void p2g_scatter_pairs(const DevParams& P, float4* __
     const bool emit = active && !absorbed;
     if (__all_sync(0xffffffffu, inside || !active)) {
         // every stencil of the warp lies in the grid: no per-node checks
-        const float h = (float)P.h;
+        const float h = P.f_h;
         const int slab = (int)P.slab, gz = P.Gz;
 #pragma unroll 1
         for (int a = 0; a < 3; a++) {
@@ -451,7 +451,7 @@ __device__ __forceinline__ void p2g_scatter_pairs(const DevParams& P, float4* __
         }
         return;
     }
-    const float h = (float)P.h;
+    const float h = P.f_h;
     const int slab = (int)P.slab, gz = P.Gz;
 #pragma unroll 1
     for (int a = 0; a < 3; a++) {
@@ -488,12 +488,12 @@ __device__ __forceinline__ void p2g_scatter_pairs(const DevParams& P, float4* __
 __device__ __forceinline__ void p2g_payload_mixed(const DevParams& P, const float E[3][3], const float C[3][3],
                                                   const float v[3], bool liquid, float Jpm1, float& mass, float mv[3],
                                                   float S[3][3]) {
-    mass = (float)(liquid ? P.liquid_mass : P.particle_mass);
+    mass = liquid ? P.f_lmass : P.f_pmass;
     float tau[3][3];
     if (liquid) {
         // kappa (1 - J^-3) with J = 1 + d: (J^3 - 1) / J^3 = d (3 + 3d + d^2) / J^3, free of cancellation
         const float J = 1.0f + Jpm1;
-        const float pw = (float)P.kappa * (Jpm1 * (3.0f + Jpm1 * (3.0f + Jpm1)) / (J * J * J));
+        const float pw = P.f_kappa * (Jpm1 * (3.0f + Jpm1 * (3.0f + Jpm1)) / (J * J * J));
 #pragma unroll
         for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -501,7 +501,7 @@ __device__ __forceinline__ void p2g_payload_mixed(const DevParams& P, const floa
     } else {
         kirchhoff_mixed(P, E, tau);
     }
-    const float dvd = (float)P.dt_vol_Dpinv;
+    const float dvd = P.f_dvd;
 #pragma unroll
     for (int i = 0; i < 3; i++) {
         mv[i] = v[i] * mass;
@@ -570,8 +570,8 @@ __device__ __forceinline__ bool fused_update_state(const DevParams& P, const Mix
                                                    int* __restrict__ rm_list, int* __restrict__ rm_count, int lane) {
     bool need_rm = false;
     if (active) {
-        const float dt = (float)P.dt;
-        const float adv = dt * (float)P.h_inv * kFixScale;
+        const float dt = P.f_dt;
+        const float adv = P.f_adv;
 #pragma unroll
         for (int d = 0; d < 3; d++) X[d] += __float2int_rn(v[d] * adv);
         float En[3][3];
@@ -651,10 +651,10 @@ __device__ __forceinline__ void fused_payload(const DevParams& P, bool active, c
         if (st & (int)kLiquid) {
             p2g_payload_mixed(P, E, C, v, true, Jpm1, mass, mv, S);
         } else {
-            mass = (float)P.particle_mass;
+            mass = P.f_pmass;
             float tau[3][3];
             tau_inv(P, inv, tau);
-            const float dvd = (float)P.dt_vol_Dpinv;
+            const float dvd = P.f_dvd;
 #pragma unroll
             for (int r = 0; r < 3; r++) {
                 mv[r] = v[r] * mass;
@@ -675,21 +675,17 @@ __device__ __forceinline__ void fused_payload(const DevParams& P, bool active, c
     }
 }
 
-// Fused G2P (this step) -> P2G (next step). do_p2g = 0 gives a plain G2P.
-// 128-thread blocks at 8 per SM (64 registers). The gather reads the warp's
-// velocity box staged in shared memory by the warp's own coalesced loads
-// (4 x kVBoxNodes float4 of dynamic shared memory); the scatter adds float4
-// atomics with same-cell particle pairs merged in registers.
+// Fused G2P (this step) -> P2G (next step) of particle i (whole warp; lanes
+// past n or disabled are inactive). do_p2g = 0 gives a plain G2P. The gather
+// reads the warp's velocity box staged in shared memory by the warp's own
+// coalesced loads (vbox: kVBoxNodes float4 of this warp); the scatter adds
+// float4 atomics with same-cell particle pairs merged in registers.
 constexpr int kVBoxNodes = 256;
-__global__ void __launch_bounds__(128, 8) k_g2p2g_mixed(DevParams P, MixedState s, int n,
-                                                        const float4* __restrict__ vel, float4* __restrict__ acc,
-                                                        int do_p2g, int record_pq, int store_vc, int* err,
-                                                        int* __restrict__ rm_list, int* __restrict__ rm_count) {
-    extern __shared__ __align__(128) float mixed_tile[];
-    __shared__ float wx_slots[3 * 128];
-    const WxSlot wx{wx_slots + threadIdx.x};
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31;
+__device__ __forceinline__ void fused_particle(const DevParams& P, const MixedState& s, int i, int n,
+                                               const float4* __restrict__ vel, float4* __restrict__ acc,
+                                               int do_p2g, int record_pq, int store_vc, int* err,
+                                               int* __restrict__ rm_list, int* __restrict__ rm_count,
+                                               float4* __restrict__ vbox, WxSlot wx, int lane) {
     bool active = i < n;
     int X[3] = {0, 0, 0}, st = (int)kDisabled;
     float E[3][3], Jpm1 = 0.f;
@@ -721,7 +717,6 @@ __global__ void __launch_bounds__(128, 8) k_g2p2g_mixed(DevParams P, MixedState 
     }
     const int st_in = st;
     const float jpm1_in = Jpm1;
-    float4* vbox = reinterpret_cast<float4*>(mixed_tile) + (threadIdx.x >> 5) * kVBoxNodes;
     g2p_gather_staged<kVBoxNodes>(P, vel, vbox, active && e0 == 0, active, base, fx, v, C, lane, wx);
     const bool need_rm = fused_update_state(P, s, i, active, X, st, st_in, jpm1_in, E, Jpm1, v, C, inv, record_pq,
                                             store_vc, rm_list, rm_count, lane);
@@ -730,6 +725,25 @@ __global__ void __launch_bounds__(128, 8) k_g2p2g_mixed(DevParams P, MixedState 
     float mass, mv[3], S[3][3];
     fused_payload(P, active, X, st, E, C, v, Jpm1, inv, base, fx, mass, mv, S, inside, err);
     p2g_scatter_pairs(P, acc, active, inside, base, fx, mass, mv, S, lane, wx);
+}
+
+// The fused kernel: 64-thread blocks at 16 per SM (64 registers, 32 warps
+// per SM), kVBoxNodes float4 of dynamic shared memory per warp. Measured on
+// the 8 M block: 0.598 ms per launch against 0.627 ms with 128-thread blocks
+// at 8 per SM (a finished warp's slot frees sooner), 0.602 ms with 32-thread
+// blocks; a persistent grid of warps looping over 32-particle chunks (static
+// or counter-scheduled) spills at 64 registers and takes 0.79-0.92 ms.
+constexpr int kFusedBlock = 64;
+__global__ void __launch_bounds__(kFusedBlock, 1024 / kFusedBlock) k_g2p2g_mixed(
+    DevParams P, MixedState s, int n, const float4* __restrict__ vel, float4* __restrict__ acc, int do_p2g,
+    int record_pq, int store_vc, int* err, int* __restrict__ rm_list, int* __restrict__ rm_count) {
+    extern __shared__ __align__(128) float mixed_tile[];
+    __shared__ float wx_slots[3 * 128];
+    const WxSlot wx{wx_slots + threadIdx.x};
+    const int lane = threadIdx.x & 31;
+    float4* vbox = reinterpret_cast<float4*>(mixed_tile) + (threadIdx.x >> 5) * kVBoxNodes;
+    fused_particle(P, s, blockIdx.x * kFusedBlock + threadIdx.x, n, vel, acc, do_p2g, record_pq, store_vc, err,
+                   rm_list, rm_count, vbox, wx, lane);
 }
 
 // Return map (FP64, mpm_kernels.cuh:486-544) of the crushed points listed by

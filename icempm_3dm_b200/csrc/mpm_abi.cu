@@ -194,6 +194,18 @@ DevParams make_dev_params(const SimParams3D& p) {
         d.fs_bpmax = (float)(beta * pmax);
         d.fs_pmax = (float)pmax;
     }
+    d.f_h = (float)p.cellsize;
+    d.f_h_inv = (float)p.cellsize_inv;
+    d.f_s4 = 4.0f * d.f_h_inv;
+    d.f_dt = (float)p.InitialTimeStep;
+    d.f_adv = d.f_dt * d.f_h_inv * kFixScale;
+    d.f_mu = (float)p.mu;
+    d.f_kappa = (float)p.kappa;
+    d.f_hkappa = (float)(0.5 * p.kappa);
+    d.f_qmu = (float)(kCoeff1 * p.mu);
+    d.f_pmass = (float)p.ParticleMass;
+    d.f_lmass = (float)p.LiquidParticleMass;
+    d.f_dvd = (float)p.dt_vol_Dpinv;
     return d;
 }
 
@@ -318,10 +330,10 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
     const int n = (int)h->n;
     if (n == 0) return MPM_OK;
     int* const rm_count = h->rm_counts + h->rm_parity;
-    // the warps' velocity boxes: 4 warps x kVBoxNodes float4 of dynamic shared memory
-    const size_t vsm = sizeof(float4) * 4 * kVBoxNodes;
-    k_g2p2g_mixed<<<blocks_for(n, 128), 128, vsm, h->stream>>>(h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g,
-                                                              record_pq, store_vc, h->err, h->rm_list, rm_count);
+    // the warps' velocity boxes: kVBoxNodes float4 of dynamic shared memory per warp
+    const size_t vsm = sizeof(float4) * (kFusedBlock / 32) * kVBoxNodes;
+    k_g2p2g_mixed<<<blocks_for(n, kFusedBlock), kFusedBlock, vsm, h->stream>>>(
+        h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g, record_pq, store_vc, h->err, h->rm_list, rm_count);
     CK_LAUNCH(h, "g2p2g mixed");
     return MPM_OK;
 }
