@@ -38,6 +38,8 @@ ENTRY_POINTS = [
     ("mpm_upload_cohesion", ctypes.c_int, [_hp, _dp, ctypes.c_uint]),
     ("mpm_download_soa", ctypes.c_int, [_hp, _dp, ctypes.c_uint, _up]),
     ("mpm_download_ids", ctypes.c_int, [_hp, _up, _up]),
+    ("mpm_upload_ids", ctypes.c_int, [_hp, _up, ctypes.c_uint]),
+    ("mpm_download_cohesion", ctypes.c_int, [_hp, _dp, _up]),
     ("mpm_sort", ctypes.c_int, [_hp]),
     ("mpm_set_sort_interval", ctypes.c_int, [_hp, ctypes.c_int]),
     ("mpm_frame_records", ctypes.c_int, [_hp, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, _up, ctypes.c_void_p, _up,
@@ -60,6 +62,25 @@ ENTRY_POINTS = [
     ("mpm_adjoint", ctypes.c_int, [_hp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp]),
     ("mpm_sort_permutation_noalloc", ctypes.c_int,
      [_pp, ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p, _up, ctypes.c_void_p]),
+    ("mpm_set_partition", ctypes.c_int, [_hp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint]),
+    ("mpm_halo_bytes", ctypes.c_size_t, [_hp]),
+    ("mpm_halo_pack", ctypes.c_int, [_hp, ctypes.c_int, ctypes.c_void_p]),
+    ("mpm_halo_add", ctypes.c_int, [_hp, ctypes.c_int, ctypes.c_void_p]),
+    ("mpm_point_record_bytes", ctypes.c_size_t, [_hp]),
+    ("mpm_points_out", ctypes.c_int, [_hp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint, _up, _up, _ip]),
+    ("mpm_points_in", ctypes.c_int, [_hp, ctypes.c_void_p, ctypes.c_uint]),
+    ("mpm_substep_p2g", ctypes.c_int, [_hp]),
+    ("mpm_substep_update_g2p", ctypes.c_int, [_hp, ctypes.c_int, _dp]),
+    ("mpm_multi_create", _hp, [_pp, ctypes.c_int, ctypes.c_uint, _ip, ctypes.c_int, _ip]),
+    ("mpm_multi_destroy", None, [_hp]),
+    ("mpm_multi_upload_soa", ctypes.c_int, [_hp, _dp, ctypes.c_uint, ctypes.c_uint, _dp]),
+    ("mpm_multi_step", ctypes.c_int, [_hp, ctypes.c_int, _dp]),
+    ("mpm_multi_download_soa", ctypes.c_int, [_hp, _dp, ctypes.c_uint, _up, _up]),
+    ("mpm_multi_rebalance", ctypes.c_int, [_hp]),
+    ("mpm_multi_info", ctypes.c_int, [_hp, ctypes.c_int, _ip, _ip, _up, _up]),
+    ("mpm_multi_stats", ctypes.c_int, [_hp, _ip, _ip, _ip]),
+    ("mpm_multi_sensors", ctypes.c_int, [_hp, _dp, _dp]),
+    ("mpm_multi_reset_indenter_force_accumulator", ctypes.c_int, [_hp]),
     ("mpm_testing_svd3x3", ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int]),
     ("mpm_testing_sizeof_params", ctypes.c_size_t, []),
     ("mpm_testing_step_timed", ctypes.c_int, [_hp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),

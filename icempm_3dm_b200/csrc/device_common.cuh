@@ -37,6 +37,11 @@ struct DevParams {
     // kappa, kappa/2, sqrt(3/2) mu, particle and liquid mass, dt V Dp^-1
     float f_h, f_h_inv, f_s4, f_dt, f_adv, f_mu, f_kappa, f_hkappa, f_qmu, f_pmass, f_lmass, f_dvd;
     double inv_gz, inv_gy;         // 1 / Gz, 1 / Gy for node index -> (x, y, z)
+    // x-slab window of a partition (GPU_Partition_3D::GridX_offset and
+    // GridX_partition; one partition: the whole grid):
+    int win_lo, win_hi;            // allowed base-node x of a particle: [x0 - halo, x0 + gxp + halo - 3]
+    int own_lo, own_hi;            // grid columns x whose contact force this partition counts
+    int node_lo, node_hi;          // node indices the update covers: slabs x0 - halo .. x0 + gxp + halo
 };
 
 // q = n / d and r = n % d for 0 <= n < 2^31 with the double reciprocal of d:
@@ -71,14 +76,15 @@ __device__ __forceinline__ void raise_error(int* err, int code) {
     if (*(volatile int*)err == 0) atomicCAS(err, 0, code);
 }
 
-// Bounds test of mpm_kernels.cuh:70-75 (one partition): the last failing
-// test of the sequence determines the code.
+// Bounds test of mpm_kernels.cuh:70-75 against the partition's window
+// (base_x - GridX_offset outside [-halo, GridX_partition + halo - 3]): the
+// last failing test of the sequence determines the code.
 __device__ __forceinline__ int stencil_error(const DevParams& P, int bx, int by, int bz) {
     int e = 0;
-    if (bx < -P.halo) e = 70;
+    if (bx < P.win_lo) e = 70;
     if (by < 0) e = 71;
     if (bz < 0) e = 72;
-    if (bx > P.Gx + P.halo - 3) e = 73;
+    if (bx > P.win_hi) e = 73;
     if (by > P.Gy - 3) e = 74;
     if (bz > P.Gz - 3) e = 75;
     return e;

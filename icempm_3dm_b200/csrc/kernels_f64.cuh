@@ -170,9 +170,9 @@ __global__ void __launch_bounds__(128, 6) k_p2g_pairs_f64(DevParams P, const dou
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_update_f64(DevParams P, double* __restrict__ grid, double ind_x, double ind_y,
                                                       double* __restrict__ sensor, double* __restrict__ force3) {
-    const long long idx = (long long)blockIdx.x * BLOCK + threadIdx.x;
+    const long long idx = (long long)P.node_lo + (long long)blockIdx.x * BLOCK + threadIdx.x;
     double f[3] = {0, 0, 0};
-    if (idx < P.nodes) {
+    if (idx < P.node_hi) {
         const double mass = grid[idx];
         if (mass != 0) {
             double v[3] = {grid[P.gstride + idx], grid[2 * P.gstride + idx], grid[3 * P.gstride + idx]};
@@ -202,17 +202,21 @@ __global__ void __launch_bounds__(BLOCK) k_update_f64(DevParams P, double* __res
                         v[0] = P.ind_velocity + vt[0];
                         v[1] = vt[1];
                         v[2] = vt[2];
+                        // a node in the overlap of two partitions is updated
+                        // by both; its force is counted by its owner only
+                        if (gx >= P.own_lo && gx < P.own_hi) {
 #pragma unroll
-                        for (int k = 0; k < 3; k++) f[k] = (prev[k] - v[k]) * mass / P.dt;
-                        float angle = atan2f((float)n0, (float)n1);
-                        angle = (float)((double)angle + MPM_PI);
-                        angle = (float)((double)angle * (P.subdiv / (2 * MPM_PI)));
-                        const int ia = min(max((int)angle, 0), P.subdiv - 1);
-                        const int iz = min(max(idx_z, 0), P.Gz - 1);
-                        double* s = sensor + 3 * (iz + ia * P.Gz);
-                        atomicAdd(s + 0, f[0]);
-                        atomicAdd(s + 1, f[1]);
-                        atomicAdd(s + 2, f[2]);
+                            for (int k = 0; k < 3; k++) f[k] = (prev[k] - v[k]) * mass / P.dt;
+                            float angle = atan2f((float)n0, (float)n1);
+                            angle = (float)((double)angle + MPM_PI);
+                            angle = (float)((double)angle * (P.subdiv / (2 * MPM_PI)));
+                            const int ia = min(max((int)angle, 0), P.subdiv - 1);
+                            const int iz = min(max(idx_z, 0), P.Gz - 1);
+                            double* s = sensor + 3 * (iz + ia * P.Gz);
+                            atomicAdd(s + 0, f[0]);
+                            atomicAdd(s + 1, f[1]);
+                            atomicAdd(s + 2, f[2]);
+                        }
                     }
                 }
             }

@@ -26,6 +26,7 @@
 #include "adjoint_f64.cuh"
 #include "sort.cuh"
 #include "frames.cuh"
+#include "partition.cuh"
 
 using namespace icempm;
 
@@ -42,10 +43,10 @@ __global__ void k_cohesion_to_apex(double* __restrict__ p0, float* __restrict__ 
     p0[i] = v;
     if (p0f) p0f[i] = (float)v;
 }
-// ids = 0, 1, ..., n-1 (the upload order)
-__global__ void k_iota(unsigned* __restrict__ ids, int n) {
+// ids = base, base + 1, ..., base + n - 1 (the upload order)
+__global__ void k_iota(unsigned* __restrict__ ids, int n, unsigned base) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) ids[i] = (unsigned)i;
+    if (i < n) ids[i] = base + (unsigned)i;
 }
 }  // namespace
 
@@ -123,6 +124,11 @@ struct mpm_handle {
     std::vector<int*> fr_scan_levels;
     bool fr_ready = false;            // a full frame has built the visual state
     cudaError_t last_cuda = cudaSuccess;
+
+    // x-slab partition (mpm_set_partition); whole grid when part_gxp == 0
+    int part_id = 0, part_x0 = 0, part_gxp = 0;
+    unsigned id_base = 0;             // upload index of particle 0 (ids are global across partitions)
+    int* xfer = nullptr;              // point transfer counters: to the left, to the right, max deviation
 };
 
 namespace {
@@ -160,6 +166,13 @@ DevParams make_dev_params(const SimParams3D& p) {
     d.inv_gz = 1.0 / (double)p.GridZ;
     d.inv_gy = 1.0 / (double)p.GridY;
     d.nodes = (long long)(p.GridXTotal + 2 * p.GridHaloSize) * d.slab;
+    // one partition: the window is the whole grid (set_window narrows it)
+    d.win_lo = -p.GridHaloSize;
+    d.win_hi = p.GridXTotal + p.GridHaloSize - 3;
+    d.own_lo = -p.GridHaloSize;
+    d.own_hi = p.GridXTotal + p.GridHaloSize;
+    d.node_lo = 0;
+    d.node_hi = (int)d.nodes;
     d.gstride = (d.nodes + 31) / 32 * 32;
     d.h = p.cellsize;
     d.h_inv = p.cellsize_inv;
@@ -222,7 +235,7 @@ void free_all(mpm_handle* h) {
     cudaFree(h->pts_alt); cudaFree(h->p0_alt); cudaFree(h->ids_alt);
     cudaFree(h->s_bucket); cudaFree(h->s_count); cudaFree(h->s_start); cudaFree(h->s_perm);
     cudaFree(h->mx); cudaFree(h->p0f); cudaFree(h->gacc); cudaFree(h->gvel);
-    cudaFree(h->rm_list); cudaFree(h->rm_counts);
+    cudaFree(h->rm_list); cudaFree(h->rm_counts); cudaFree(h->xfer);
     for (double* c : h->ckpt) cudaFree(c);
     for (double* c : h->seg) cudaFree(c);
     h->ckpt.clear();
@@ -299,14 +312,14 @@ int launch_p2g(mpm_handle* h) {
 }
 
 int launch_update(mpm_handle* h, double ind_x, double ind_y, double* force3) {
+    // the nodes of the partition's window (one partition: the whole grid)
+    const unsigned nb = blocks_for((long long)h->dp.node_hi - h->dp.node_lo, 256);
     if (is_mixed(h)) {
-        k_update_mixed<256><<<blocks_for(h->dp.nodes, 256), 256, 0, h->stream>>>(h->dp, h->gacc, h->gvel, ind_x, ind_y,
-                                                                                 h->sensor, force3);
+        k_update_mixed<256><<<nb, 256, 0, h->stream>>>(h->dp, h->gacc, h->gvel, ind_x, ind_y, h->sensor, force3);
         CK_LAUNCH(h, "update mixed");
         return MPM_OK;
     }
-    k_update_f64<256><<<blocks_for(h->dp.nodes, 256), 256, 0, h->stream>>>(h->dp, h->grid, ind_x, ind_y, h->sensor,
-                                                                             force3);
+    k_update_f64<256><<<nb, 256, 0, h->stream>>>(h->dp, h->grid, ind_x, ind_y, h->sensor, force3);
     CK_LAUNCH(h, "update kernel");
     return MPM_OK;
 }
@@ -360,7 +373,14 @@ int reset_grid(mpm_handle* h) {
         h->p2g_ready = false;
         return MPM_OK;
     }
-    CK(h, cudaMemsetAsync(h->grid, 0, sizeof(double) * 4 * (size_t)h->dp.gstride, h->stream));
+    if (h->dp.node_lo == 0 && h->dp.node_hi == h->dp.nodes) {
+        CK(h, cudaMemsetAsync(h->grid, 0, sizeof(double) * 4 * (size_t)h->dp.gstride, h->stream));
+        return MPM_OK;
+    }
+    // a partition clears its window's slabs of the 4 arrays
+    const size_t cnt = (size_t)(h->dp.node_hi - h->dp.node_lo);
+    for (int c = 0; c < 4; c++)
+        CK(h, cudaMemsetAsync(h->grid + c * h->dp.gstride + h->dp.node_lo, 0, sizeof(double) * cnt, h->stream));
     return MPM_OK;
 }
 
@@ -597,7 +617,7 @@ int mpm_upload_soa(mpm_handle* h, const double* soa, unsigned pitch, unsigned n)
     if (n) {
         CK(h, cudaMemcpy2DAsync(h->pts, sizeof(double) * h->pitch, soa, sizeof(double) * pitch, sizeof(double) * n,
                                 MPM_N_PTS_ARRAYS, cudaMemcpyHostToDevice, h->stream));
-        k_iota<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->ids, (int)n);
+        k_iota<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->ids, (int)n, h->id_base);
         CK_LAUNCH(h, "ids");
         CK(h, cudaStreamSynchronize(h->stream));   // soa may be released when the call returns
     }
@@ -662,6 +682,30 @@ int mpm_download_ids(mpm_handle* h, unsigned* ids, unsigned* n) {
     if (h->n) CK(h, cudaMemcpyAsync(ids, h->ids, sizeof(unsigned) * h->n, cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
     if (n) *n = h->n;
+    return MPM_OK;
+}
+
+int mpm_upload_ids(mpm_handle* h, const unsigned* ids, unsigned n) {
+    if (!h || (!ids && n)) return MPM_ERR_ARG;
+    if (!h->uploaded) return MPM_ERR_STATE;
+    if (n != h->n) return MPM_ERR_ARG;
+    if (n) {
+        CK(h, cudaMemcpyAsync(h->ids, ids, sizeof(unsigned) * n, cudaMemcpyHostToDevice, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+    }
+    return MPM_OK;
+}
+
+int mpm_download_cohesion(mpm_handle* h, double* cohesion, unsigned* n) {
+    if (!h || !cohesion || !n) return MPM_ERR_ARG;
+    if (!h->p0) return MPM_ERR_STATE;
+    std::vector<double> p0(h->n);
+    if (h->n) {
+        CK(h, cudaMemcpyAsync(p0.data(), h->p0, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+    }
+    for (unsigned i = 0; i < h->n; i++) cohesion[i] = p0[i] * h->prms.DP_tan_phi;
+    *n = h->n;
     return MPM_OK;
 }
 
@@ -925,6 +969,742 @@ int mpm_count(mpm_handle* h, unsigned* n) {
 }
 
 const char* mpm_last_error_string(void) { return g_last_error; }
+
+}  // extern "C"
+
+// ------------------------------------------------- x-slab partitions
+//
+// GPU_Implementation6 with nPartitions > 1 (gpu_implementation6.cpp:31-208,
+// 340-382, model_3d.cpp:35-108): each partition is a handle that owns a slab
+// of grid columns [x0, x0 + gxp) and the particles split to it; after P2G the
+// partitions add each other's 2 * halo boundary slabs, and every
+// UpdateEveryNthStep / PointTransferFrequency substeps the particles that
+// left a slab move to the neighbour.
+
+namespace {
+
+size_t halo_nodes(const mpm_handle* h) { return (size_t)2 * h->prms.GridHaloSize * (size_t)h->dp.slab; }
+
+// node offset of the first halo slab on a side of the window: columns
+// x0 - halo (left) or x0 + gxp - halo (right), i.e. array slabs x0, x0 + gxp
+long long halo_offset(const mpm_handle* h, int side) {
+    const int x0 = h->part_x0, gxp = h->part_gxp ? h->part_gxp : h->prms.GridXTotal;
+    return (long long)(side ? x0 + gxp : x0) * h->dp.slab;
+}
+
+size_t record_bytes(const mpm_handle* h) { return (is_mixed(h) ? sizeof(unsigned) : sizeof(double)) * kRecWords; }
+
+}  // namespace
+
+extern "C" {
+
+int mpm_set_partition(mpm_handle* h, int id, int x0, int gxp, unsigned id_base) {
+    if (!h || id < 0 || id > 255 || x0 < 0 || gxp < 1 || x0 + gxp > h->prms.GridXTotal) return MPM_ERR_ARG;
+    const SimParams3D& p = h->prms;
+    const bool whole = x0 == 0 && gxp == p.GridXTotal;
+    if (!whole && p.GridHaloSize < 3) return MPM_ERR_ARG;   // a stencil spans 3 columns
+    const int halo = p.GridHaloSize;
+    h->part_id = id;
+    h->part_x0 = x0;
+    h->part_gxp = gxp;
+    h->id_base = id_base;
+    h->dp.win_lo = x0 - halo;
+    h->dp.win_hi = x0 + gxp + halo - 3;
+    h->dp.own_lo = x0 == 0 ? -halo : x0;
+    h->dp.own_hi = x0 + gxp == p.GridXTotal ? p.GridXTotal + halo : x0 + gxp;
+    h->dp.node_lo = (int)((long long)x0 * h->dp.slab);
+    h->dp.node_hi = (int)((long long)(x0 + gxp + 2 * halo) * h->dp.slab);
+    if (!h->xfer) CK(h, cudaMalloc(&h->xfer, sizeof(int) * 3));
+    return MPM_OK;
+}
+
+size_t mpm_halo_bytes(const mpm_handle* h) {
+    if (!h) return 0;
+    return halo_nodes(h) * (is_mixed(h) ? sizeof(float4) : 4 * sizeof(double));
+}
+
+int mpm_halo_pack(mpm_handle* h, int side, void* dst) {
+    if (!h || !dst || (side != 0 && side != 1)) return MPM_ERR_ARG;
+    const size_t hn = halo_nodes(h);
+    if (!hn) return MPM_OK;
+    const long long off = halo_offset(h, side);
+    if (is_mixed(h)) {
+        CK(h, cudaMemcpyAsync(dst, h->gacc + off, sizeof(float4) * hn, cudaMemcpyDeviceToDevice, h->stream));
+        return MPM_OK;
+    }
+    double* d = static_cast<double*>(dst);
+    for (int c = 0; c < 4; c++)
+        CK(h, cudaMemcpyAsync(d + c * hn, h->grid + c * h->dp.gstride + off, sizeof(double) * hn,
+                              cudaMemcpyDeviceToDevice, h->stream));
+    return MPM_OK;
+}
+
+int mpm_halo_add(mpm_handle* h, int side, const void* src) {
+    if (!h || !src || (side != 0 && side != 1)) return MPM_ERR_ARG;
+    const size_t hn = halo_nodes(h);
+    if (!hn) return MPM_OK;
+    const long long off = halo_offset(h, side);
+    if (is_mixed(h))
+        k_halo_add_f4<<<blocks_for(hn, 256), 256, 0, h->stream>>>(h->gacc, off, (int)hn,
+                                                                  static_cast<const float4*>(src));
+    else
+        k_halo_add_f64<<<blocks_for(hn, 256), 256, 0, h->stream>>>(h->grid, h->dp.gstride, off, (int)hn,
+                                                                   static_cast<const double*>(src));
+    CK_LAUNCH(h, "halo add");
+    return MPM_OK;
+}
+
+size_t mpm_point_record_bytes(const mpm_handle* h) { return h ? record_bytes(h) : 0; }
+
+int mpm_points_out(mpm_handle* h, void* left, void* right, unsigned capacity, unsigned* n_left, unsigned* n_right,
+                   int* max_deviation) {
+    if (!h || !n_left || !n_right || (capacity && (!left || !right))) return MPM_ERR_ARG;
+    if (!h->uploaded) return MPM_ERR_STATE;
+    if (!h->xfer) CK(h, cudaMalloc(&h->xfer, sizeof(int) * 3));
+    CK(h, cudaMemsetAsync(h->xfer, 0, sizeof(int) * 3, h->stream));
+    const SimParams3D& p = h->prms;
+    XferGeom G;
+    G.x0 = h->part_x0;
+    G.gxp = h->part_gxp ? h->part_gxp : p.GridXTotal;
+    G.keep_track = p.GridHaloSize / 2 - 1;
+    G.cap = (int)std::min<unsigned>(capacity, 0x7fffffff);
+    G.left_ok = G.x0 > 0 && capacity > 0;
+    G.right_ok = G.x0 + G.gxp < p.GridXTotal && capacity > 0;
+    G.h_inv = p.cellsize_inv;
+    const int n = (int)h->n;
+    if (n) {
+        if (is_mixed(h))
+            k_points_out_mixed<<<blocks_for(n, 256), 256, 0, h->stream>>>(
+                G, static_cast<unsigned*>(h->mx), h->pitch, h->p0, h->ids, n, static_cast<unsigned*>(left),
+                static_cast<unsigned*>(right), h->xfer);
+        else
+            k_points_out_f64<<<blocks_for(n, 256), 256, 0, h->stream>>>(G, h->pts, h->pitch, h->p0, h->ids, n,
+                                                                        static_cast<double*>(left),
+                                                                        static_cast<double*>(right), h->xfer);
+        CK_LAUNCH(h, "points out");
+    }
+    int c[3] = {0, 0, 0};
+    CK(h, cudaMemcpyAsync(c, h->xfer, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    *n_left = (unsigned)std::min(c[0], G.cap);
+    *n_right = (unsigned)std::min(c[1], G.cap);
+    if (max_deviation) *max_deviation = c[2];
+    return MPM_OK;
+}
+
+int mpm_points_in(mpm_handle* h, const void* records, unsigned count) {
+    if (!h || (count && !records)) return MPM_ERR_ARG;
+    if (!h->uploaded) return MPM_ERR_STATE;
+    if (!count) return MPM_OK;
+    if ((size_t)h->n + count > h->capacity) return MPM_ERR_RECEIVE;   // mpm_kernels.cuh:420
+    if (is_mixed(h))
+        k_points_in_mixed<<<blocks_for(count, 256), 256, 0, h->stream>>>(
+            static_cast<unsigned*>(h->mx), h->pitch, h->p0, h->p0f, h->ids, (int)h->n, (int)count,
+            static_cast<const unsigned*>(records));
+    else
+        k_points_in_f64<<<blocks_for(count, 256), 256, 0, h->stream>>>(h->pts, h->pitch, h->p0, h->ids, (int)h->n,
+                                                                       (int)count,
+                                                                       static_cast<const double*>(records));
+    CK_LAUNCH(h, "points in");
+    h->n += count;
+    h->fr_ready = false;
+    return MPM_OK;
+}
+
+}  // extern "C"
+
+// The two halves of a partitioned substep, around the halo exchange.
+// First: the P2G sums of the current state in the grid (FP64: the window
+// cleared and P2G; mixed: already there from the previous substep's fused
+// kernel, else a standalone P2G).
+int substep_p2g(mpm_handle* h) {
+    int r;
+    if (is_mixed(h)) {
+        if (!h->p2g_ready) {
+            if ((r = reset_grid(h)) || (r = launch_p2g(h))) return r;
+            h->p2g_ready = true;
+        }
+        return MPM_OK;
+    }
+    if ((r = reset_grid(h)) || (r = launch_p2g(h))) return r;
+    return MPM_OK;
+}
+
+// Second: node update at the indenter position of the substep, G2P (mixed:
+// fused with the next substep's P2G, then the return map of the points that
+// crushed); force3 (device) accumulates the substep's force.
+int substep_update_g2p(mpm_handle* h, double ind_x, double ind_y, int record, int store_vc, double* force3) {
+    int r;
+    if ((r = launch_update(h, ind_x, ind_y, force3))) return r;
+    if (is_mixed(h)) {
+        if ((r = launch_g2p2g_mixed(h, 1, record, store_vc))) return r;
+        return launch_return_map_mixed(h, 1);
+    }
+    return launch_g2p(h, record);
+}
+
+extern "C" {
+
+int mpm_substep_p2g(mpm_handle* h) {
+    if (!h) return MPM_ERR_ARG;
+    if (!h->uploaded) return MPM_ERR_STATE;
+    return substep_p2g(h);
+}
+
+int mpm_substep_update_g2p(mpm_handle* h, int store_vc, double force3[3]) {
+    if (!h) return MPM_ERR_ARG;
+    if (!h->uploaded) return MPM_ERR_STATE;
+    SimParams3D& p = h->prms;
+    p.SimulationTime += p.InitialTimeStep;
+    p.indenter_x = p.indenter_x_initial + p.SimulationTime * p.IndVelocity;
+    const int record = (p.SimulationStep % p.UpdateEveryNthStep) == 0;
+    CK(h, cudaMemsetAsync(h->force_phase, 0, sizeof(double) * 3, h->stream));
+    int r = substep_update_g2p(h, p.indenter_x, p.indenter_y, record, store_vc, h->force_phase);
+    if (r) return r;
+    p.SimulationStep += 1;
+    if (force3) {
+        CK(h, cudaMemcpyAsync(force3, h->force_phase, sizeof(double) * 3, cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+    }
+    return MPM_OK;
+}
+
+}  // extern "C"
+
+// -------------------------------------- partitions driven in one process
+
+struct mpm_multi {
+    SimParams3D prms;
+    int precision = MPM_PRECISION_FP64;
+    int np = 0;
+    unsigned capacity = 0;            // particles per partition
+    unsigned xfer_cap = 0;            // records per direction (VectorCapacity_transfer)
+    bool cohesion = false;
+    std::vector<mpm_handle*> part;
+    std::vector<unsigned> disabled;   // nPts_disabled of each partition
+    // per partition, on its device: halo send buffers (left, right), halo
+    // receive buffers, point-record out buffers (left, right) and an in buffer
+    std::vector<void*> hsend[2], hrecv[2], pout[2], pin;
+    std::vector<cudaEvent_t> ev_packed, ev_received, ev_out;
+    int max_deviation = 0;
+    int max_sent = 0;
+    int rebalances = 0;
+    std::vector<double> force;        // per-substep force of the running step call, summed over partitions
+};
+
+namespace {
+
+void multi_free(mpm_multi* m) {
+    for (int i = 0; i < (int)m->part.size(); i++) {
+        mpm_handle* h = m->part[i];
+        if (!h) continue;
+        cudaSetDevice(h->device);
+        for (int s = 0; s < 2; s++) {
+            if (i < (int)m->hsend[s].size()) cudaFree(m->hsend[s][i]);
+            if (i < (int)m->hrecv[s].size()) cudaFree(m->hrecv[s][i]);
+            if (i < (int)m->pout[s].size()) cudaFree(m->pout[s][i]);
+        }
+        if (i < (int)m->pin.size()) cudaFree(m->pin[i]);
+        if (i < (int)m->ev_packed.size()) cudaEventDestroy(m->ev_packed[i]);
+        if (i < (int)m->ev_received.size()) cudaEventDestroy(m->ev_received[i]);
+        if (i < (int)m->ev_out.size()) cudaEventDestroy(m->ev_out[i]);
+        mpm_destroy(h);
+    }
+    m->part.clear();
+}
+
+// ProxyPoint3D::getCellIndex / getXIndex (proxypoint3d.cpp:158-170)
+inline long long cell_key(const SimParams3D& p, double x, double y, double z) {
+    return (long long)(int)(x * p.cellsize_inv + 0.5) * p.GridY * p.GridZ + (long long)(int)(y * p.cellsize_inv + 0.5) * p.GridZ +
+           (int)(z * p.cellsize_inv + 0.5);
+}
+inline int x_index(const SimParams3D& p, double x) { return (int)(x * p.cellsize_inv + 0.5); }
+
+inline bool disabled_word(double u) {
+    long long v;
+    std::memcpy(&v, &u, sizeof(v));
+    return (v & MPM_STATUS_DISABLED) == MPM_STATUS_DISABLED;
+}
+
+// HostSideSOA::RemoveDisabledAndSort (host_side_soa.cpp:56-67) as a stable
+// sort: the order of the kept particles, by cell key.
+std::vector<unsigned> sorted_order(const SimParams3D& p, const double* soa, size_t pitch, unsigned n) {
+    std::vector<unsigned> idx;
+    idx.reserve(n);
+    for (unsigned i = 0; i < n; i++)
+        if (!disabled_word(soa[i])) idx.push_back(i);
+    std::vector<long long> key(n);
+    for (unsigned i : idx)
+        key[i] = cell_key(p, soa[MPM_POSX * pitch + i], soa[(MPM_POSX + 1) * pitch + i], soa[(MPM_POSX + 2) * pitch + i]);
+    std::stable_sort(idx.begin(), idx.end(), [&](unsigned a, unsigned b) { return key[a] < key[b]; });
+    return idx;
+}
+
+// split_hssoa_into_partitions (gpu_implementation6.cpp:340-382) of a sorted
+// SoA (n particles, row stride pitch) and its upload: partition i takes
+// (n - done) / (np - i) particles; its slab ends at the x index of the first
+// particle of the next one; the partition id goes into bits 24-31 of each
+// particle's status word (ProxyPoint3D::setPartition, proxypoint3d.cpp:89-110).
+// ids: the global id of each particle (may be null: 0, 1, ...).
+int multi_split_upload(mpm_multi* m, std::vector<double>& soa, size_t pitch, unsigned n, const double* cohesion,
+                       const std::vector<unsigned>* ids) {
+    const SimParams3D& p = m->prms;
+    std::vector<int> x0(m->np), cnt(m->np);
+    unsigned done = 0;
+    int off = 0;
+    for (int i = 0; i < m->np; i++) {
+        cnt[i] = (int)((n - done) / (unsigned)(m->np - i));
+        x0[i] = off;
+        if (i < m->np - 1) {
+            const unsigned first_next = done + (unsigned)cnt[i];
+            off = first_next < n ? x_index(p, soa[MPM_POSX * pitch + first_next]) : p.GridXTotal;
+            off = std::max(off, x0[i] + 1);
+            off = std::min(off, p.GridXTotal - (m->np - 1 - i));
+        }
+        for (unsigned j = done; j < done + (unsigned)cnt[i]; j++) {
+            long long v;
+            std::memcpy(&v, &soa[j], sizeof(v));
+            v &= 0xffffffff00ffffffLL;
+            v |= (long long)i << 24;
+            std::memcpy(&soa[j], &v, sizeof(v));
+        }
+        done += (unsigned)cnt[i];
+    }
+    done = 0;
+    for (int i = 0; i < m->np; i++) {
+        mpm_handle* h = m->part[i];
+        const int gxp = (i < m->np - 1 ? x0[i + 1] : p.GridXTotal) - x0[i];
+        if ((unsigned)cnt[i] > h->capacity) return MPM_ERR_CAPACITY;
+        int r = mpm_set_partition(h, i, x0[i], gxp, done);
+        if (r) return r;
+        // the partition's particles as a SoA of their own (28 rows of cnt[i])
+        std::vector<double> local((size_t)MPM_N_PTS_ARRAYS * std::max(cnt[i], 1));
+        for (int row = 0; row < MPM_N_PTS_ARRAYS; row++)
+            std::memcpy(&local[(size_t)row * cnt[i]], &soa[row * pitch + done], sizeof(double) * cnt[i]);
+        if ((r = mpm_upload_soa(h, local.data(), (unsigned)cnt[i], (unsigned)cnt[i]))) return r;
+        if (cohesion && (r = mpm_upload_cohesion(h, cohesion + done, (unsigned)cnt[i]))) return r;
+        if (ids && cnt[i]) {
+            CK(h, cudaMemcpyAsync(h->ids, ids->data() + done, sizeof(unsigned) * cnt[i], cudaMemcpyHostToDevice,
+                                  h->stream));
+            CK(h, cudaStreamSynchronize(h->stream));
+        }
+        m->disabled[i] = 0;
+        done += (unsigned)cnt[i];
+    }
+    return MPM_OK;
+}
+
+// the halo exchange after P2G (gpu_implementation6.cpp:31-112): every
+// partition packs its boundary slabs; each receives its neighbours' packed
+// slabs of the same columns (a peer copy when they live on another device)
+// and adds them (partition_kernel_receive_halos_*). Events order the
+// streams; a send buffer is packed again only after both neighbours copied it.
+int multi_halo_exchange(mpm_multi* m) {
+    const int np = m->np;
+    if (np < 2) return MPM_OK;
+    for (int i = 0; i < np; i++) {
+        mpm_handle* h = m->part[i];
+        CK(h, cudaSetDevice(h->device));
+        if (i > 0) CK(h, cudaStreamWaitEvent(h->stream, m->ev_received[i - 1], 0));
+        if (i < np - 1) CK(h, cudaStreamWaitEvent(h->stream, m->ev_received[i + 1], 0));
+        int r;
+        if (i > 0 && (r = mpm_halo_pack(h, 0, m->hsend[0][i]))) return r;
+        if (i < np - 1 && (r = mpm_halo_pack(h, 1, m->hsend[1][i]))) return r;
+        CK(h, cudaEventRecord(m->ev_packed[i], h->stream));
+    }
+    for (int i = 0; i < np; i++) {
+        mpm_handle* h = m->part[i];
+        CK(h, cudaSetDevice(h->device));
+        const size_t bytes = mpm_halo_bytes(h);
+        if (i > 0) {
+            mpm_handle* l = m->part[i - 1];
+            CK(h, cudaStreamWaitEvent(h->stream, m->ev_packed[i - 1], 0));
+            CK(h, cudaMemcpyPeerAsync(m->hrecv[0][i], h->device, m->hsend[1][i - 1], l->device, bytes, h->stream));
+        }
+        if (i < np - 1) {
+            mpm_handle* rr = m->part[i + 1];
+            CK(h, cudaStreamWaitEvent(h->stream, m->ev_packed[i + 1], 0));
+            CK(h, cudaMemcpyPeerAsync(m->hrecv[1][i], h->device, m->hsend[0][i + 1], rr->device, bytes, h->stream));
+        }
+        CK(h, cudaEventRecord(m->ev_received[i], h->stream));
+        int r;
+        if (i > 0 && (r = mpm_halo_add(h, 0, m->hrecv[0][i]))) return r;
+        if (i < np - 1 && (r = mpm_halo_add(h, 1, m->hrecv[1][i]))) return r;
+    }
+    return MPM_OK;
+}
+
+// GPU_Implementation6::receive_points (gpu_implementation6.cpp:135-208): the
+// records each partition wrote for its neighbours are copied to them and
+// appended to their particle lists.
+int multi_transfer_points(mpm_multi* m) {
+    const int np = m->np;
+    if (np < 2) return MPM_OK;
+    std::vector<unsigned> nl(np), nr(np);
+    for (int i = 0; i < np; i++) {
+        mpm_handle* h = m->part[i];
+        CK(h, cudaSetDevice(h->device));
+        int dev = 0;
+        int r = mpm_points_out(h, m->pout[0][i], m->pout[1][i], m->xfer_cap, &nl[i], &nr[i], &dev);
+        if (r) return r;
+        m->max_deviation = std::max(m->max_deviation, dev);
+        m->max_sent = std::max(m->max_sent, (int)std::max(nl[i], nr[i]));
+        m->disabled[i] += nl[i] + nr[i];
+        CK(h, cudaEventRecord(m->ev_out[i], h->stream));
+    }
+    const size_t rb = record_bytes(m->part[0]);
+    for (int i = 0; i < np; i++) {
+        mpm_handle* h = m->part[i];
+        CK(h, cudaSetDevice(h->device));
+        unsigned k = 0;
+        // from the left neighbour (its right-going records), then from the right
+        if (i > 0 && nr[i - 1]) {
+            CK(h, cudaStreamWaitEvent(h->stream, m->ev_out[i - 1], 0));
+            CK(h, cudaMemcpyPeerAsync(m->pin[i], h->device, m->pout[1][i - 1], m->part[i - 1]->device,
+                                      rb * nr[i - 1], h->stream));
+            k += nr[i - 1];
+        }
+        if (i < np - 1 && nl[i + 1]) {
+            CK(h, cudaStreamWaitEvent(h->stream, m->ev_out[i + 1], 0));
+            CK(h, cudaMemcpyPeerAsync(static_cast<char*>(m->pin[i]) + rb * k, h->device, m->pout[0][i + 1],
+                                      m->part[i + 1]->device, rb * nl[i + 1], h->stream));
+            k += nl[i + 1];
+        }
+        int r = mpm_points_in(h, m->pin[i], k);
+        if (r) return r;
+    }
+    // the out buffers are written again at the next transfer only after
+    // every receiver's copy: wait for them here (transfers are rare)
+    for (int i = 0; i < np; i++) {
+        mpm_handle* h = m->part[i];
+        CK(h, cudaSetDevice(h->device));
+        CK(h, cudaStreamSynchronize(h->stream));
+    }
+    return MPM_OK;
+}
+
+int multi_download(mpm_multi* m, std::vector<double>& soa, std::vector<unsigned>& ids,
+                   std::vector<double>& cohesion, unsigned& n) {
+    n = 0;
+    for (mpm_handle* h : m->part) n += h->n;
+    soa.assign((size_t)MPM_N_PTS_ARRAYS * std::max(n, 1u), 0.0);
+    ids.assign(std::max(n, 1u), 0u);
+    cohesion.assign(m->cohesion ? std::max(n, 1u) : 0, 0.0);
+    unsigned off = 0;
+    std::vector<double> local;
+    for (mpm_handle* h : m->part) {
+        CK(h, cudaSetDevice(h->device));
+        const unsigned k = h->n;
+        local.assign((size_t)MPM_N_PTS_ARRAYS * std::max(k, 1u), 0.0);
+        unsigned got = 0;
+        int r = mpm_download_soa(h, local.data(), std::max(k, 1u), &got);
+        if (r) return r;
+        for (int row = 0; row < MPM_N_PTS_ARRAYS; row++)
+            std::memcpy(&soa[(size_t)row * n + off], &local[(size_t)row * std::max(k, 1u)], sizeof(double) * k);
+        if ((r = mpm_download_ids(h, ids.data() + off, &got))) return r;
+        if (m->cohesion && k) {
+            CK(h, cudaMemcpyAsync(cohesion.data() + off, h->p0, sizeof(double) * k, cudaMemcpyDeviceToHost,
+                                  h->stream));
+            CK(h, cudaStreamSynchronize(h->stream));
+            for (unsigned j = 0; j < k; j++) cohesion[off + j] *= h->prms.DP_tan_phi;   // back to c = p0 tan(phi)
+        }
+        off += k;
+    }
+    return MPM_OK;
+}
+
+// Model3D::Step's rebalance (model_3d.cpp:99-108): all particles back to the
+// host, RemoveDisabledAndSort, split again, upload.
+int multi_rebalance(mpm_multi* m) {
+    std::vector<double> soa, coh;
+    std::vector<unsigned> ids;
+    unsigned n = 0;
+    int r = multi_download(m, soa, ids, coh, n);
+    if (r) return r;
+    const std::vector<unsigned> order = sorted_order(m->prms, soa.data(), n, n);
+    const unsigned k = (unsigned)order.size();
+    std::vector<double> s2((size_t)MPM_N_PTS_ARRAYS * std::max(k, 1u));
+    std::vector<double> c2(m->cohesion ? std::max(k, 1u) : 0);
+    std::vector<unsigned> i2(std::max(k, 1u));
+    for (unsigned j = 0; j < k; j++) {
+        const unsigned src = order[j];
+        for (int row = 0; row < MPM_N_PTS_ARRAYS; row++) s2[(size_t)row * k + j] = soa[(size_t)row * n + src];
+        if (m->cohesion) c2[j] = coh[src];
+        i2[j] = ids[src];
+    }
+    m->rebalances++;
+    return multi_split_upload(m, s2, k, k, m->cohesion ? c2.data() : nullptr, &i2);
+}
+
+bool multi_needs_rebalance(const mpm_multi* m) {
+    const SimParams3D& p = m->prms;
+    for (int i = 0; i < m->np; i++) {
+        const mpm_handle* h = m->part[i];
+        const double n = std::max<double>(h->n, 1.0);
+        const double free_share = ((double)h->capacity - (double)h->n) / n;
+        const double disabled_share = (double)m->disabled[i] / (double)h->capacity;
+        if (free_share < p.RebalanceThresholdFreeSpaceRemaining) return true;
+        if (disabled_share > p.RebalanceThresholdDisabledPercentage) return true;
+    }
+    return false;
+}
+
+}  // namespace
+
+extern "C" {
+
+mpm_multi* mpm_multi_create(const SimParams3D* prms, int precision, unsigned capacity, const int* devices,
+                            int ndevices, int* status) {
+    int st = MPM_OK;
+    mpm_multi* m = nullptr;
+    do {
+        if (!params_valid(prms) || prms->nPartitions < 1 || prms->nPartitions > 256 || !devices || ndevices < 1 ||
+            capacity == 0) {
+            st = MPM_ERR_ARG;
+            break;
+        }
+        if (prms->nPartitions > 1 && prms->GridHaloSize < 3) { st = MPM_ERR_ARG; break; }
+        m = new (std::nothrow) mpm_multi();
+        if (!m) { st = MPM_ERR_ARG; break; }
+        m->prms = *prms;
+        m->precision = precision;
+        m->np = prms->nPartitions;
+        m->capacity = capacity;
+        m->xfer_cap = (unsigned)std::max(prms->VectorCapacity_transfer, 1);
+        m->disabled.assign(m->np, 0);
+        for (int s = 0; s < 2; s++) {
+            m->hsend[s].assign(m->np, nullptr);
+            m->hrecv[s].assign(m->np, nullptr);
+            m->pout[s].assign(m->np, nullptr);
+        }
+        m->pin.assign(m->np, nullptr);
+        for (int i = 0; i < m->np && st == MPM_OK; i++) {
+            // GPU_Implementation6::initialize: partition i on device i % count
+            mpm_handle* h = mpm_create(prms, precision, capacity, devices[i % ndevices], &st);
+            if (!h) break;
+            m->part.push_back(h);
+            cudaSetDevice(h->device);
+            const size_t hb = mpm_halo_bytes(h), rb = record_bytes(h) * m->xfer_cap;
+            cudaEvent_t e[3];
+            for (int k = 0; k < 3; k++)
+                if (cudaEventCreateWithFlags(&e[k], cudaEventDisableTiming) != cudaSuccess) st = MPM_ERR_CUDA;
+            m->ev_packed.push_back(e[0]);
+            m->ev_received.push_back(e[1]);
+            m->ev_out.push_back(e[2]);
+            for (int s = 0; s < 2 && st == MPM_OK; s++) {
+                if (cudaMalloc(&m->hsend[s][i], std::max<size_t>(hb, 16)) != cudaSuccess ||
+                    cudaMalloc(&m->hrecv[s][i], std::max<size_t>(hb, 16)) != cudaSuccess ||
+                    cudaMalloc(&m->pout[s][i], rb) != cudaSuccess)
+                    st = MPM_ERR_CUDA;
+            }
+            if (st == MPM_OK && cudaMalloc(&m->pin[i], 2 * rb) != cudaSuccess) st = MPM_ERR_CUDA;
+            // the events start out recorded, so the first waits on them pass
+            for (int k = 0; k < 3 && st == MPM_OK; k++)
+                if (cudaEventRecord(e[k], h->stream) != cudaSuccess) st = MPM_ERR_CUDA;
+        }
+        if (st != MPM_OK) break;
+        // GPU_Implementation6::enable_peer_access: neighbours on other devices
+        for (int i = 0; i + 1 < m->np; i++) {
+            const int a = m->part[i]->device, b = m->part[i + 1]->device;
+            if (a == b) continue;
+            int ok = 0;
+            cudaDeviceCanAccessPeer(&ok, a, b);
+            if (ok) {
+                cudaSetDevice(a);
+                cudaDeviceEnablePeerAccess(b, 0);
+                cudaSetDevice(b);
+                cudaDeviceEnablePeerAccess(a, 0);
+                cudaGetLastError();   // "already enabled" is not an error here
+            }
+        }
+    } while (0);
+    if (status) *status = st;
+    if (st != MPM_OK) {
+        if (m) { multi_free(m); delete m; }
+        return nullptr;
+    }
+    return m;
+}
+
+void mpm_multi_destroy(mpm_multi* m) {
+    if (!m) return;
+    for (mpm_handle* h : m->part) {
+        cudaSetDevice(h->device);
+        cudaStreamSynchronize(h->stream);
+    }
+    multi_free(m);
+    delete m;
+}
+
+int mpm_multi_upload_soa(mpm_multi* m, const double* soa, unsigned pitch, unsigned n, const double* cohesion) {
+    if (!m || (!soa && n) || pitch < n) return MPM_ERR_ARG;
+    const std::vector<unsigned> order = sorted_order(m->prms, soa, pitch, n);
+    const unsigned k = (unsigned)order.size();
+    std::vector<double> s2((size_t)MPM_N_PTS_ARRAYS * std::max(k, 1u));
+    std::vector<double> c2(cohesion ? std::max(k, 1u) : 0);
+    std::vector<unsigned> ids(std::max(k, 1u));
+    for (unsigned j = 0; j < k; j++) {
+        for (int row = 0; row < MPM_N_PTS_ARRAYS; row++) s2[(size_t)row * k + j] = soa[(size_t)row * pitch + order[j]];
+        if (cohesion) c2[j] = cohesion[order[j]];
+        ids[j] = order[j];
+    }
+    m->cohesion = cohesion != nullptr;
+    m->max_deviation = 0;
+    return multi_split_upload(m, s2, k, k, cohesion ? c2.data() : nullptr, &ids);
+}
+
+int mpm_multi_step(mpm_multi* m, int nsteps, double* force_hist) {
+    if (!m || nsteps < 0) return MPM_ERR_ARG;
+    for (mpm_handle* h : m->part)
+        if (!h->uploaded) return MPM_ERR_STATE;
+    if (nsteps == 0) return MPM_OK;
+    SimParams3D& p = m->prms;
+    for (mpm_handle* h : m->part) {
+        CK(h, cudaSetDevice(h->device));
+        if (nsteps > h->force_steps_cap) {
+            CK(h, cudaStreamSynchronize(h->stream));
+            cudaFree(h->force_steps);
+            h->force_steps = nullptr;
+            CK(h, cudaMalloc(&h->force_steps, sizeof(double) * 3 * (size_t)nsteps));
+            h->force_steps_cap = nsteps;
+        }
+        CK(h, cudaMemsetAsync(h->force_steps, 0, sizeof(double) * 3 * (size_t)nsteps, h->stream));
+    }
+    std::vector<double> total((size_t)3 * nsteps, 0.0);
+    int done = 0;           // substeps whose forces are in the handles' buffers since the last flush
+    auto flush_forces = [&](int upto) -> int {
+        std::vector<double> f((size_t)3 * nsteps);
+        for (mpm_handle* h : m->part) {
+            CK(h, cudaSetDevice(h->device));
+            CK(h, cudaMemcpyAsync(f.data(), h->force_steps, sizeof(double) * 3 * (size_t)upto, cudaMemcpyDeviceToHost,
+                                  h->stream));
+            CK(h, cudaStreamSynchronize(h->stream));
+            for (int k = 3 * done; k < 3 * upto; k++) total[k] += f[k];
+        }
+        done = upto;
+        return MPM_OK;
+    };
+    const int per = std::max(1, p.UpdateEveryNthStep / std::max(1, p.PointTransferFrequency));
+    for (int s = 0; s < nsteps; s++) {
+        p.SimulationTime += p.InitialTimeStep;
+        p.indenter_x = p.indenter_x_initial + p.SimulationTime * p.IndVelocity;
+        const int record = (p.SimulationStep % p.UpdateEveryNthStep) == 0;
+        const bool transfer = m->np > 1 && (p.SimulationStep % per) == 0;
+        const bool last = s == nsteps - 1;
+        // v and C reach the mixed state (the fused chain keeps them in
+        // registers) where a download can follow: the call's last substep,
+        // a point transfer, an animation frame's end (a possible rebalance)
+        const bool frame_end = (p.SimulationStep + 1) % p.UpdateEveryNthStep == 0;
+        int r;
+        for (mpm_handle* h : m->part) {
+            CK(h, cudaSetDevice(h->device));
+            if ((r = substep_p2g(h))) return r;
+        }
+        if ((r = multi_halo_exchange(m))) return r;
+        for (mpm_handle* h : m->part) {
+            CK(h, cudaSetDevice(h->device));
+            if ((r = substep_update_g2p(h, p.indenter_x, p.indenter_y, record, last || transfer || frame_end,
+                                        h->force_steps + 3 * s)))
+                return r;
+        }
+        p.SimulationStep += 1;
+        if (transfer && (r = multi_transfer_points(m))) return r;
+        if (p.SimulationStep % p.UpdateEveryNthStep == 0) {
+            // the end of an animation frame (model_3d.cpp:72-108): transfer
+            // more often if a point strayed past half the halo; rebalance
+            // when a partition runs short of room or holds many holes
+            if (m->max_deviation > p.GridHaloSize / 2) p.PointTransferFrequency++;
+            m->max_deviation = 0;
+            if (m->np > 1 && multi_needs_rebalance(m)) {
+                if ((r = flush_forces(s + 1))) return r;
+                if ((r = multi_rebalance(m))) return r;
+            }
+        }
+    }
+    if (int r = flush_forces(nsteps)) return r;
+    if (force_hist) std::memcpy(force_hist, total.data(), sizeof(double) * 3 * nsteps);
+    int code = 0;
+    for (mpm_handle* h : m->part) {
+        h->prms.SimulationTime = p.SimulationTime;
+        h->prms.SimulationStep = p.SimulationStep;
+        h->prms.indenter_x = p.indenter_x;
+        h->prms.PointTransferFrequency = p.PointTransferFrequency;
+        CK(h, cudaSetDevice(h->device));
+        int c = 0;
+        int r2 = read_error(h, &c);
+        if (r2) return r2;
+        if (c && !code) code = c;
+    }
+    return code;
+}
+
+int mpm_multi_download_soa(mpm_multi* m, double* soa, unsigned pitch, unsigned* ids, unsigned* n) {
+    if (!m || !n) return MPM_ERR_ARG;
+    std::vector<double> all, coh;
+    std::vector<unsigned> id;
+    unsigned k = 0;
+    int r = multi_download(m, all, id, coh, k);
+    if (r) return r;
+    *n = k;
+    if (!soa) return MPM_OK;
+    if (pitch < k) return MPM_ERR_ARG;
+    for (int row = 0; row < MPM_N_PTS_ARRAYS; row++)
+        std::memcpy(soa + (size_t)row * pitch, all.data() + (size_t)row * k, sizeof(double) * k);
+    if (ids) std::memcpy(ids, id.data(), sizeof(unsigned) * k);
+    return MPM_OK;
+}
+
+int mpm_multi_rebalance(mpm_multi* m) {
+    if (!m) return MPM_ERR_ARG;
+    return multi_rebalance(m);
+}
+
+int mpm_multi_info(mpm_multi* m, int i, int* x0, int* gxp, unsigned* n, unsigned* n_disabled) {
+    if (!m || i < 0 || i >= m->np) return MPM_ERR_ARG;
+    const mpm_handle* h = m->part[i];
+    if (x0) *x0 = h->part_x0;
+    if (gxp) *gxp = h->part_gxp;
+    if (n) *n = h->n;
+    if (n_disabled) *n_disabled = m->disabled[i];
+    return MPM_OK;
+}
+
+int mpm_multi_stats(mpm_multi* m, int* max_sent, int* rebalances, int* point_transfer_frequency) {
+    if (!m) return MPM_ERR_ARG;
+    if (max_sent) *max_sent = m->max_sent;
+    if (rebalances) *rebalances = m->rebalances;
+    if (point_transfer_frequency) *point_transfer_frequency = m->prms.PointTransferFrequency;
+    return MPM_OK;
+}
+
+int mpm_multi_sensors(mpm_multi* m, double* sensor, double total[3]) {
+    if (!m) return MPM_ERR_ARG;
+    const size_t ns = sensor_count(m->prms);
+    std::vector<double> acc(ns, 0.0), one(ns);
+    double t[3] = {0, 0, 0};
+    for (mpm_handle* h : m->part) {
+        CK(h, cudaSetDevice(h->device));
+        double tt[3];
+        int r = mpm_sensors(h, one.data(), tt);
+        if (r) return r;
+        for (size_t j = 0; j < ns; j++) acc[j] += one[j];
+        for (int k = 0; k < 3; k++) t[k] += tt[k];
+    }
+    if (sensor) std::memcpy(sensor, acc.data(), sizeof(double) * ns);
+    if (total)
+        for (int k = 0; k < 3; k++) total[k] = t[k];
+    return MPM_OK;
+}
+
+int mpm_multi_reset_indenter_force_accumulator(mpm_multi* m) {
+    if (!m) return MPM_ERR_ARG;
+    for (mpm_handle* h : m->part) {
+        CK(h, cudaSetDevice(h->device));
+        int r = mpm_reset_indenter_force_accumulator(h);
+        if (r) return r;
+    }
+    return MPM_OK;
+}
 
 }  // extern "C"
 

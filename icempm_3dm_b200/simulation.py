@@ -86,6 +86,52 @@ class MPMHandle:
     def sort(self):
         return check(LIB.mpm_sort(self._h), "mpm_sort")
 
+    def upload_ids(self, ids):
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        check(LIB.mpm_upload_ids(self._h, uptr(ids), ids.size), "mpm_upload_ids")
+
+    def cohesion(self):
+        n = self.count()
+        c = np.zeros(max(n, 1))
+        nn = ctypes.c_uint(0)
+        check(LIB.mpm_download_cohesion(self._h, dptr(c), ctypes.byref(nn)), "mpm_download_cohesion")
+        return c[:nn.value]
+
+    # -- x-slab partition (one partition of a partitioned run)
+    def set_partition(self, pid, x0, gxp, id_base=0):
+        check(LIB.mpm_set_partition(self._h, int(pid), int(x0), int(gxp), int(id_base)), "mpm_set_partition")
+
+    def halo_bytes(self):
+        return int(LIB.mpm_halo_bytes(self._h))
+
+    def halo_pack(self, side, dst_ptr):
+        check(LIB.mpm_halo_pack(self._h, int(side), ctypes.c_void_p(dst_ptr)), "mpm_halo_pack")
+
+    def halo_add(self, side, src_ptr):
+        check(LIB.mpm_halo_add(self._h, int(side), ctypes.c_void_p(src_ptr)), "mpm_halo_add")
+
+    def record_bytes(self):
+        return int(LIB.mpm_point_record_bytes(self._h))
+
+    def points_out(self, left_ptr, right_ptr, capacity):
+        """(records to the left, to the right, max deviation in columns)."""
+        nl, nr, dev = ctypes.c_uint(0), ctypes.c_uint(0), ctypes.c_int(0)
+        check(LIB.mpm_points_out(self._h, ctypes.c_void_p(left_ptr), ctypes.c_void_p(right_ptr), int(capacity),
+                                 ctypes.byref(nl), ctypes.byref(nr), ctypes.byref(dev)), "mpm_points_out")
+        return nl.value, nr.value, dev.value
+
+    def points_in(self, src_ptr, count):
+        check(LIB.mpm_points_in(self._h, ctypes.c_void_p(src_ptr), int(count)), "mpm_points_in")
+
+    def substep_p2g(self):
+        check(LIB.mpm_substep_p2g(self._h), "mpm_substep_p2g")
+
+    def substep_update_g2p(self, store_vc, want_force=True):
+        f = np.zeros(3)
+        check(LIB.mpm_substep_update_g2p(self._h, int(store_vc), dptr(f) if want_force else None),
+              "mpm_substep_update_g2p")
+        return f
+
     def frame_records(self, frame, full):
         """mpm_frame_records: the VisualPoint records (full) or the
         (UpdatePos, UpdateJp, UpdateStatus) records of this frame."""

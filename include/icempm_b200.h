@@ -132,6 +132,12 @@ int  mpm_download_soa(mpm_handle* h, double* soa, unsigned pitch, unsigned* n);
 /* New: the upload index of each particle in the current order (the sort of
  * mpm_sort permutes particles; this gives the permutation). */
 int  mpm_download_ids(mpm_handle* h, unsigned* ids, unsigned* n);
+/* New: replaces the ids of the n particles the handle holds (n must be its
+ * count), e.g. with global indices of a partitioned run. */
+int  mpm_upload_ids(mpm_handle* h, const unsigned* ids, unsigned n);
+/* New: the per-particle cohesion c_i (p0_i * DP_tan_phi) in the handle's
+ * current order; MPM_ERR_STATE when none was uploaded. */
+int  mpm_download_cohesion(mpm_handle* h, double* cohesion, unsigned* n);
 /* HostSideSOA::RemoveDisabledAndSort (host_side_soa.cpp:56-67) on the device:
  * drops disabled particles and orders the rest by the cell key of
  * ProxyPoint3D::getCellIndex (proxypoint3d.cpp:158-163), stable (ties keep
@@ -217,6 +223,129 @@ int  mpm_synchronize(mpm_handle* h);
 int  mpm_get_params(mpm_handle* h, SimParams3D* out);
 /* Number of particles currently held (after sorts that drop disabled ones). */
 int  mpm_count(mpm_handle* h, unsigned* n);
+/* ------------------------------------------------ x-slab partitions
+ * nPartitions > 1: the particles are split into slabs of grid columns along
+ * x; after P2G neighbouring partitions add each other's 2*GridHaloSize
+ * boundary slabs, and particles that leave a slab move to the neighbour.
+ * Each partition keeps a grid of the whole domain and works on its window
+ * of it (the same node indices in every partition). GridHaloSize >= 3. */
+
+/* GPU_Partition_3D's slab (GPU_Implementation6::split_hssoa_into_partitions,
+ * gpu_implementation6.cpp:340-382): partition `id` (0..255) owns the grid
+ * columns [x0, x0 + gxp) of GridXTotal and works on them with GridHaloSize
+ * halo columns on each side. Particles are checked against base x in
+ * [x0 - halo, x0 + gxp + halo - 3] (70 / 73 outside), the node update covers
+ * the window's columns, and the indenter force of a node is counted by the
+ * partition that owns its column only (the first and the last partition
+ * also own the halo columns beyond the grid's ends); the reference, whose
+ * partitions update their overlap alike, adds the overlap nodes' force of
+ * both partitions (gpu_implementation6.cpp:450-455). id_base: the upload
+ * index the next mpm_upload_soa gives its first particle (ids are global
+ * across partitions). x0 = 0, gxp = GridXTotal is the one-partition default. */
+int  mpm_set_partition(mpm_handle* h, int id, int x0, int gxp, unsigned id_base);
+/* Bytes of one side's halo: 2*GridHaloSize*GridY*GridZ nodes, 32 B each
+ * (FP64: 4 arrays) or 16 B (mixed: the float4 accumulator). */
+size_t mpm_halo_bytes(const mpm_handle* h);
+/* The halo sends of GPU_Implementation6::p2g (gpu_implementation6.cpp:31-77):
+ * copies the P2G sums of the 2*GridHaloSize columns around the window's left
+ * (side 0: x0 - halo .. x0 + halo - 1) or right (side 1: x0 + gxp - halo ..
+ * x0 + gxp + halo - 1) boundary into the device buffer dst (mpm_halo_bytes;
+ * FP64: the 4 arrays one after another). */
+int  mpm_halo_pack(mpm_handle* h, int side, void* dst);
+/* partition_kernel_receive_halos_left (mpm_kernels.cuh:103-118) and
+ * partition_kernel_receive_halos_right (:120-135): adds a neighbour's packed
+ * slabs of the same columns (its side 1 for our side 0 and vice versa) into
+ * this grid. Addition commutes, so both partitions then hold equal sums. */
+int  mpm_halo_add(mpm_handle* h, int side, const void* src);
+/* Bytes of one particle record of a point transfer: 256 (FP64: the 28 SoA
+ * rows, the apex shift p0, the id) or 128 (mixed: the 28 rows of the mixed
+ * state, p0, the id). */
+size_t mpm_point_record_bytes(const mpm_handle* h);
+/* The point transfer of partition_kernel_g2p (mpm_kernels.cuh:353-398) and
+ * PreparePointForTransfer (:401-408), run after a G2P: a particle whose base x
+ * lies more than 3 columns left of x0, or right of x0 + gxp, is copied as a
+ * record into left / right (device buffers of `capacity` records each) and
+ * disabled (its status word set to the disabled bit). Only sides with a
+ * neighbour (x0 > 0; x0 + gxp < GridXTotal) send. *n_left, *n_right: the
+ * records written (at most capacity: a particle beyond a full buffer stays,
+ * as in the reference); *max_deviation (may be NULL): the largest distance in
+ * columns of a particle beyond the slab by more than halo/2 - 1 columns
+ * (the reference's idx_pts_max_extent). Waits for the device. */
+int  mpm_points_out(mpm_handle* h, void* left, void* right, unsigned capacity, unsigned* n_left, unsigned* n_right,
+                    int* max_deviation);
+/* partition_kernel_receive_points (mpm_kernels.cuh:411-427): appends `count`
+ * records (device buffer) after the handle's particles; MPM_ERR_RECEIVE (5)
+ * if they do not fit in its capacity. */
+int  mpm_points_in(mpm_handle* h, const void* records, unsigned count);
+
+/* The two halves of a substep of one partition, for a driver that runs the
+ * halo exchange between them itself (one partition per process).
+ * mpm_substep_p2g: the P2G sums of the current state in the grid (the first
+ * half of GPU_Implementation6::p2g, gpu_implementation6.cpp:31-77; FP64:
+ * window cleared, P2G; mixed: computed by the previous substep's fused
+ * kernel, else a standalone P2G). */
+int  mpm_substep_p2g(mpm_handle* h);
+/* The rest of the substep of Model3D::Step (model_3d.cpp:24-112, the loop at
+ * :35-51): SimulationTime += dt, the indenter moves, node update, G2P (mixed:
+ * fused with the next substep's P2G), SimulationStep += 1. store_vc (mixed):
+ * write v and C to the state (needed before a download or a point transfer).
+ * force3 (host, may be NULL: no wait) receives the substep's force of the
+ * nodes this partition owns. */
+int  mpm_substep_update_g2p(mpm_handle* h, int store_vc, double force3[3]);
+
+/* GPU_Implementation6 with prms->nPartitions partitions in one process:
+ * GPU_Implementation6::initialize (gpu_implementation6.cpp:319-337) puts
+ * partition i on devices[i % ndevices]; GPU_Implementation6::allocate_arrays
+ * (:385-401) with `capacity` particles per partition (nPtsTotal /
+ * nPartitions * (1 + ExtraSpaceForIncomingPoints) in the reference) and
+ * VectorCapacity_transfer records per direction;
+ * GPU_Implementation6::enable_peer_access (:219-315) for neighbours on other
+ * devices. */
+typedef struct mpm_multi mpm_multi;
+mpm_multi* mpm_multi_create(const SimParams3D* prms, int precision, unsigned capacity, const int* devices,
+                            int ndevices, int* status);
+void mpm_multi_destroy(mpm_multi* m);
+/* HostSideSOA::RemoveDisabledAndSort (host_side_soa.cpp:56-67), as a
+ * stable sort here, then GPU_Implementation6::split_hssoa_into_partitions
+ * (gpu_implementation6.cpp:340-382) and
+ * GPU_Implementation6::transfer_ponts_to_device (gpu_implementation6.cpp:404-414)
+ * of a host SoA in the HostSideSOA row layout: partition i takes
+ * [n - done] / [N - i] particles, its slab ends at the x index of the next
+ * partition's first particle, and bits 24-31 of the status word get i.
+ * cohesion (may be NULL) as mpm_upload_cohesion. The upload index of each
+ * particle is its id. */
+int  mpm_multi_upload_soa(mpm_multi* m, const double* soa, unsigned pitch, unsigned n, const double* cohesion);
+/* Model3D::Step (model_3d.cpp:24-112) for nsteps substeps: per substep P2G,
+ * the halo exchange (GPU_Implementation6::p2g, gpu_implementation6.cpp:31-77;
+ * GPU_Implementation6::receive_halos, :80-112), the node update, G2P, and
+ * every UpdateEveryNthStep / PointTransferFrequency substeps the point
+ * transfer (GPU_Implementation6::receive_points, :135-208); at the end of
+ * each animation frame PointTransferFrequency grows when a particle strayed
+ * more than GridHaloSize/2 columns, and the partitions are rebalanced
+ * (RemoveDisabledAndSort, split, upload; model_3d.cpp:76-108) when one has
+ * less than RebalanceThresholdFreeSpaceRemaining of free room or more than
+ * RebalanceThresholdDisabledPercentage of its capacity disabled.
+ * force_hist: nsteps x 3 forces summed over the partitions. */
+int  mpm_multi_step(mpm_multi* m, int nsteps, double* force_hist);
+/* GPU_Implementation6::transfer_from_device (gpu_implementation6.cpp:417-496):
+ * the partitions' particles one after another (disabled ones included), row
+ * stride pitch, and (ids may be NULL) the upload index of each; *n = count.
+ * soa = NULL only returns the count. */
+int  mpm_multi_download_soa(mpm_multi* m, double* soa, unsigned pitch, unsigned* ids, unsigned* n);
+/* The rebalance of Model3D::Step (model_3d.cpp:24-112, the rebalance at
+ * :99-108) on request. */
+int  mpm_multi_rebalance(mpm_multi* m);
+/* Partition i's slab [x0, x0 + gxp), its particle count (disabled included)
+ * and its disabled count since the last split (nPts_disabled). */
+int  mpm_multi_info(mpm_multi* m, int i, int* x0, int* gxp, unsigned* n, unsigned* n_disabled);
+/* The largest transfer of one partition to one side, the rebalances so far
+ * and the current PointTransferFrequency. */
+int  mpm_multi_stats(mpm_multi* m, int* max_sent, int* rebalances, int* point_transfer_frequency);
+/* mpm_sensors summed over the partitions. */
+int  mpm_multi_sensors(mpm_multi* m, double* sensor, double total[3]);
+/* mpm_reset_indenter_force_accumulator on every partition. */
+int  mpm_multi_reset_indenter_force_accumulator(mpm_multi* m);
+
 /* ---------------------------------------------------------------- adjoint
  * No counterpart in the reference (new, for calibrating ice strength).
  * Reverse-mode gradients of a loss on the indenter force history with
