@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="block8m")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--accum", default="float", choices=["float", "fixed"],
+                    help="mixed P2G grid accumulation: FP32 float4 atomics or 64-bit fixed point")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-arm", action="store_true", help="skip the plain FP64 step on the same block")
     ap.add_argument("--fp64-steps", type=int, default=300, help="substeps of the FP64 arm (at most --steps)")
@@ -343,6 +345,8 @@ def run_ours(args):
 
     h = MPMHandle(prms, n, prec, device=local)
     h.set_stream(stream.cuda_stream)
+    if args.accum == "fixed":
+        h.set_grid_accumulation(1)
     h.upload(soa, cohesion=coh)
     h.sort()
     h.step(max(args.warmup, 3), want_forces=False)
@@ -402,6 +406,8 @@ def run_ours(args):
     out_host = torch.empty(soa.shape, dtype=torch.float64, pin_memory=True).numpy()
     h2 = MPMHandle(prms, n, prec, device=local)
     h2.set_stream(stream.cuda_stream)
+    if args.accum == "fixed":
+        h2.set_grid_accumulation(1)
     h2.upload(host_np, cohesion=coh)
     h2.sort()
     h2.step(3, want_forces=False)
@@ -445,6 +451,7 @@ def run_ours(args):
             "dtype": "f32+f64" if prec == PRECISION_MIXED else "f64",
             "data": "synthetic: seeded jittered-lattice ice block (shapes of the target configuration)",
             "config": {"workload": args.workload, "particles": n, "precision": args.precision,
+                       "grid_accumulation": args.accum if prec == PRECISION_MIXED else "fp64",
                        "grid": [prms.GridXTotal, prms.GridY, prms.GridZ], "h": prms.cellsize,
                        "dt": prms.InitialTimeStep, "parallelism": f"replicas x{world}",
                        "l2": "state larger than L2 (no flush needed)",

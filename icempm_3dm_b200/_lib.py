@@ -42,6 +42,7 @@ ENTRY_POINTS = [
     ("mpm_download_cohesion", ctypes.c_int, [_hp, _dp, _up]),
     ("mpm_sort", ctypes.c_int, [_hp]),
     ("mpm_set_sort_interval", ctypes.c_int, [_hp, ctypes.c_int]),
+    ("mpm_set_grid_accumulation", ctypes.c_int, [_hp, ctypes.c_int]),
     ("mpm_frame_records", ctypes.c_int, [_hp, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, _up, ctypes.c_void_p, _up,
                                          ctypes.c_void_p, _up, ctypes.c_void_p, _up]),
     ("mpm_reset_grid", ctypes.c_int, [_hp]),

@@ -36,6 +36,9 @@ struct DevParams {
     // every thread): h, 1/h, 4/h, dt, dt/h 2^20 (fixed-point advection), mu,
     // kappa, kappa/2, sqrt(3/2) mu, particle and liquid mass, dt V Dp^-1
     float f_h, f_h_inv, f_s4, f_dt, f_adv, f_mu, f_kappa, f_hkappa, f_qmu, f_pmass, f_lmass, f_dvd;
+    // scales of the fixed-point grid accumulator (AccQ) and their inverses
+    float f_qm, f_qp;
+    double q_inv_m, q_inv_p;
     double inv_gz, inv_gy;         // 1 / Gz, 1 / Gy for node index -> (x, y, z)
     // x-slab window of a partition (GPU_Partition_3D::GridX_offset and
     // GridX_partition; one partition: the whole grid):

@@ -348,10 +348,41 @@ __device__ __noinline__ ElasticState return_map_f64(const DPParams P, const Elas
 
 // ------------------------------------------------------------- P2G part
 
+// The grid accumulator of the mixed P2G (and of the halo exchange):
+//   AccF4: float4 {m, m v} per node, added with FP32 vector atomics (the
+//          default): the sum's rounding depends on the order of the adds;
+//   AccQ:  4 int64 per node, each contribution converted to fixed point with
+//          the per-quantity scales q_m = 2^44 / m_ref and q_p = 2^44 /
+//          (m_ref vmax) (m_ref = the larger particle mass) and added as an
+//          integer: the sum is exact and independent of the order, so a run
+//          repeats bit for bit. Resolution 2^-44 m_ref in mass and
+//          2^-44 m_ref vmax in momentum; a node holds 2^19 such full-scale
+//          contributions before the 2^63 range (each conversion saturates).
+struct AccF4 {
+    float4* a;
+    __device__ __forceinline__ void add(const DevParams&, int node, float m, float x, float y, float z) const {
+        atomicAdd(a + node, make_float4(m, x, y, z));
+    }
+};
+struct AccQ {
+    unsigned long long* a;   // 4 per node: m, m vx, m vy, m vz in units of 1 / scale
+    __device__ __forceinline__ static unsigned long long q(float v, float scale) {
+        const float t = fminf(fmaxf(v * scale, -4.0e18f), 4.0e18f);
+        return (unsigned long long)__float2ll_rn(t);
+    }
+    __device__ __forceinline__ void add(const DevParams& P, int node, float m, float x, float y, float z) const {
+        unsigned long long* p = a + 4 * (size_t)node;
+        atomicAdd(p + 0, q(m, P.f_qm));
+        atomicAdd(p + 1, q(x, P.f_qp));
+        atomicAdd(p + 2, q(y, P.f_qp));
+        atomicAdd(p + 3, q(z, P.f_qp));
+    }
+};
+
 // Scatter of one particle (base, fx, m, mv, S) with the warp reduction over
 // lanes sharing a base cell; leaders add float4 {m, mv} to acc.
-template <bool AGG = true>
-__device__ __forceinline__ void p2g_scatter_mixed(const DevParams& P, float4* __restrict__ acc, bool active, bool inside,
+template <bool AGG, class Acc>
+__device__ __forceinline__ void p2g_scatter_mixed(const DevParams& P, Acc acc, bool active, bool inside,
                                                   const int base[3], const float fx[3], float mass, const float mv[3],
                                                   const float S[3][3], int lane) {
     const int i0 = ((base[0] + P.halo) * P.Gy + base[1]) * P.Gz + base[2];
@@ -392,7 +423,7 @@ __device__ __forceinline__ void p2g_scatter_mixed(const DevParams& P, float4* __
                 }
                 if (!active || lane != leader) continue;
                 if (!inside && !node_inside(P, base[0] + a, base[1] + b, base[2] + c)) continue;
-                atomicAdd(acc + (ib + c), make_float4(val[0], val[1], val[2], val[3]));
+                acc.add(P, ib + c, val[0], val[1], val[2], val[3]);
             }
         }
     }
@@ -404,7 +435,8 @@ __device__ __forceinline__ void p2g_scatter_mixed(const DevParams& P, float4* __
 // even-ranked lane, which issues the single float4 atomic for both. A third
 // particle of a cell (rank 2) pairs with a fourth or adds alone. Halves the
 // atomic traffic to L2 at ppc ~2 for 8 shuffles and adds per node.
-__device__ __forceinline__ void p2g_scatter_pairs(const DevParams& P, float4* __restrict__ acc, bool active,
+template <class Acc>
+__device__ __forceinline__ void p2g_scatter_pairs(const DevParams& P, Acc acc, bool active,
                                                   bool inside, const int base[3], const float fx[3], float mass,
                                                   const float mv[3], const float S[3][3], int lane, WxSlot wx) {
     const int i0 = ((base[0] + P.halo) * P.Gy + base[1]) * P.Gz + base[2];
@@ -445,7 +477,7 @@ __device__ __forceinline__ void p2g_scatter_pairs(const DevParams& P, float4* __
                         const float o = __shfl_down_sync(0xffffffffu, val[q], 1);
                         if (absorb) val[q] += o;
                     }
-                    if (emit) atomicAdd(acc + (ib + c), make_float4(val[0], val[1], val[2], val[3]));
+                    if (emit) acc.add(P, ib + c, val[0], val[1], val[2], val[3]);
                 }
             }
         }
@@ -478,7 +510,7 @@ __device__ __forceinline__ void p2g_scatter_pairs(const DevParams& P, float4* __
                 }
                 if (!active || absorbed) continue;
                 if (!inside && !node_inside(P, base[0] + a, base[1] + b, base[2] + c)) continue;
-                atomicAdd(acc + (ib + c), make_float4(val[0], val[1], val[2], val[3]));
+                acc.add(P, ib + c, val[0], val[1], val[2], val[3]);
             }
         }
     }
@@ -522,7 +554,8 @@ __device__ __forceinline__ void load_mixed(const MixedState& s, int i, int X[3],
 }
 
 // Standalone P2G from the stored state (first step, phase API).
-__global__ void __launch_bounds__(256) k_p2g_mixed(DevParams P, MixedState s, int n, float4* __restrict__ acc,
+template <class Acc>
+__global__ void __launch_bounds__(256) k_p2g_mixed(DevParams P, MixedState s, int n, Acc acc,
                                                    int* err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -554,7 +587,7 @@ __global__ void __launch_bounds__(256) k_p2g_mixed(DevParams P, MixedState s, in
 #pragma unroll
             for (int c = 0; c < 3; c++) S[r][c] = 0.f;
     }
-    p2g_scatter_mixed(P, acc, active, inside, base, fx, mass, mv, S, lane);
+    p2g_scatter_mixed<true>(P, acc, active, inside, base, fx, mass, mv, S, lane);
 }
 
 // G2P tail of the fused kernels for one particle (whole warp): fixed-point
@@ -681,8 +714,9 @@ __device__ __forceinline__ void fused_payload(const DevParams& P, bool active, c
 // coalesced loads (vbox: kVBoxNodes float4 of this warp); the scatter adds
 // float4 atomics with same-cell particle pairs merged in registers.
 constexpr int kVBoxNodes = 256;
+template <class Acc>
 __device__ __forceinline__ void fused_particle(const DevParams& P, const MixedState& s, int i, int n,
-                                               const float4* __restrict__ vel, float4* __restrict__ acc,
+                                               const float4* __restrict__ vel, Acc acc,
                                                int do_p2g, int record_pq, int store_vc, int* err,
                                                int* __restrict__ rm_list, int* __restrict__ rm_count,
                                                float4* __restrict__ vbox, WxSlot wx, int lane) {
@@ -734,8 +768,9 @@ __device__ __forceinline__ void fused_particle(const DevParams& P, const MixedSt
 // blocks; a persistent grid of warps looping over 32-particle chunks (static
 // or counter-scheduled) spills at 64 registers and takes 0.79-0.92 ms.
 constexpr int kFusedBlock = 64;
+template <class Acc>
 __global__ void __launch_bounds__(kFusedBlock, 1024 / kFusedBlock) k_g2p2g_mixed(
-    DevParams P, MixedState s, int n, const float4* __restrict__ vel, float4* __restrict__ acc, int do_p2g,
+    DevParams P, MixedState s, int n, const float4* __restrict__ vel, Acc acc, int do_p2g,
     int record_pq, int store_vc, int* err, int* __restrict__ rm_list, int* __restrict__ rm_count) {
     extern __shared__ __align__(128) float mixed_tile[];
     __shared__ float wx_slots[3 * 128];
@@ -750,9 +785,10 @@ __global__ void __launch_bounds__(kFusedBlock, 1024 / kFusedBlock) k_g2p2g_mixed
 // k_g2p2g_mixed, then their P2G (direct float4 atomics) when do_p2g. The
 // list holds *count indices; the kernel also clears next_count, the counter
 // the next fused launch appends to. Grid-stride over the list.
+template <class Acc>
 __global__ void __launch_bounds__(128) k_return_map_mixed(DevParams P, MixedState s, const int* __restrict__ rm_list,
                                                           const int* __restrict__ count, int* __restrict__ next_count,
-                                                          float4* __restrict__ acc, int do_p2g, int* err) {
+                                                          Acc acc, int do_p2g, int* err) {
     if (blockIdx.x == 0 && threadIdx.x == 0) *next_count = 0;
     const int m = *count;
     const int lane = threadIdx.x & 31;
@@ -793,23 +829,45 @@ __global__ void __launch_bounds__(128) k_return_map_mixed(DevParams P, MixedStat
 // reciprocal of the mass), contact force in FP64 (sensor and per-substep
 // total), velocities written as float4, the accumulator cleared for the next
 // P2G. Node coordinates by reciprocal multiplication (no integer division).
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_update_mixed(DevParams P, float4* __restrict__ acc, float4* __restrict__ vel,
+// The node's sums {m, m vx, m vy, m vz} in double, and the accumulator
+// cleared for the next P2G (when the node has mass).
+__device__ __forceinline__ void take_node(AccF4 acc, const DevParams&, int idx, double& m, double mv[3]) {
+    const float4 a = acc.a[idx];
+    m = a.x;
+    mv[0] = a.y;
+    mv[1] = a.z;
+    mv[2] = a.w;
+    if (m != 0) acc.a[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+__device__ __forceinline__ void take_node(AccQ acc, const DevParams& P, int idx, double& m, double mv[3]) {
+    ulonglong2* p = reinterpret_cast<ulonglong2*>(acc.a + 4 * (size_t)idx);
+    const ulonglong2 q0 = p[0], q1 = p[1];
+    m = (double)(long long)q0.x * P.q_inv_m;
+    mv[0] = (double)(long long)q0.y * P.q_inv_p;
+    mv[1] = (double)(long long)q1.x * P.q_inv_p;
+    mv[2] = (double)(long long)q1.y * P.q_inv_p;
+    if (q0.x != 0) {
+        p[0] = make_ulonglong2(0ull, 0ull);
+        p[1] = make_ulonglong2(0ull, 0ull);
+    }
+}
+
+template <int BLOCK, class Acc>
+__global__ void __launch_bounds__(BLOCK) k_update_mixed(DevParams P, Acc acc, float4* __restrict__ vel,
                                                         double ind_x, double ind_y, double* __restrict__ sensor,
                                                         double* __restrict__ force3) {
     const int idx = P.node_lo + blockIdx.x * BLOCK + threadIdx.x;   // the handle keeps nodes < 2^31
     double f[3] = {0, 0, 0};
     if (idx < P.node_hi) {
-        const float4 a = acc[idx];
-        const double mass = a.x;
+        double mass, amv[3];
+        take_node(acc, P, idx, mass, amv);
         if (mass != 0) {
-            acc[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
             int idx_z, idx_y;
             const int col = div_by(idx, P.Gz, P.inv_gz, idx_z);
             const int idx_x = div_by(col, P.Gy, P.inv_gy, idx_y);
             const int gx = idx_x - P.halo, gy = idx_y, gz = idx_z;
             const double inv_m = 1.0 / mass;
-            double v[3] = {(double)a.y * inv_m, (double)a.z * inv_m, (double)a.w * inv_m};
+            double v[3] = {amv[0] * inv_m, amv[1] * inv_m, amv[2] * inv_m};
             v[1] -= P.dt_gravity;
             const double vsq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
             if (vsq > P.vmax_sq) {

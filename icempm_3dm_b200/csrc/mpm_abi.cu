@@ -91,6 +91,7 @@ struct mpm_handle {
     void* mx = nullptr;
     float* p0f = nullptr;
     float4* gacc = nullptr;
+    unsigned long long* gacc_q = nullptr;   // the fixed-point accumulator when selected (4 per node)
     float4* gvel = nullptr;
     bool p2g_ready = false;           // gacc holds the P2G of the current state
     int num_sms = 148;
@@ -219,6 +220,17 @@ DevParams make_dev_params(const SimParams3D& p) {
     d.f_pmass = (float)p.ParticleMass;
     d.f_lmass = (float)p.LiquidParticleMass;
     d.f_dvd = (float)p.dt_vol_Dpinv;
+    {   // fixed-point accumulator scales: 2^44 units per reference mass and
+        // per reference momentum (the larger particle mass at vmax)
+        double m_ref = std::max(p.ParticleMass, p.LiquidParticleMass);
+        if (!(m_ref > 0)) m_ref = 1.0;
+        const double v_ref = p.vmax > 0 ? p.vmax : 1.0;
+        const double two44 = 17592186044416.0;
+        d.f_qm = (float)(two44 / m_ref);
+        d.f_qp = (float)(two44 / (m_ref * v_ref));
+        d.q_inv_m = 1.0 / (double)d.f_qm;
+        d.q_inv_p = 1.0 / (double)d.f_qp;
+    }
     return d;
 }
 
@@ -234,7 +246,7 @@ void free_all(mpm_handle* h) {
     cudaFree(h->force_steps); cudaFree(h->force_phase); cudaFree(h->err);
     cudaFree(h->pts_alt); cudaFree(h->p0_alt); cudaFree(h->ids_alt);
     cudaFree(h->s_bucket); cudaFree(h->s_count); cudaFree(h->s_start); cudaFree(h->s_perm);
-    cudaFree(h->mx); cudaFree(h->p0f); cudaFree(h->gacc); cudaFree(h->gvel);
+    cudaFree(h->mx); cudaFree(h->p0f); cudaFree(h->gacc); cudaFree(h->gvel); cudaFree(h->gacc_q);
     cudaFree(h->rm_list); cudaFree(h->rm_counts); cudaFree(h->xfer);
     for (double* c : h->ckpt) cudaFree(c);
     for (double* c : h->seg) cudaFree(c);
@@ -302,7 +314,10 @@ int launch_p2g(mpm_handle* h) {
     const int n = (int)h->n;
     if (n == 0) return MPM_OK;
     if (is_mixed(h)) {
-        k_p2g_mixed<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->dp, mixed_state(h), n, h->gacc, h->err);
+        if (h->gacc_q)
+            k_p2g_mixed<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->dp, mixed_state(h), n, AccQ{h->gacc_q}, h->err);
+        else
+            k_p2g_mixed<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->dp, mixed_state(h), n, AccF4{h->gacc}, h->err);
         CK_LAUNCH(h, "p2g mixed");
         return MPM_OK;
     }
@@ -315,7 +330,12 @@ int launch_update(mpm_handle* h, double ind_x, double ind_y, double* force3) {
     // the nodes of the partition's window (one partition: the whole grid)
     const unsigned nb = blocks_for((long long)h->dp.node_hi - h->dp.node_lo, 256);
     if (is_mixed(h)) {
-        k_update_mixed<256><<<nb, 256, 0, h->stream>>>(h->dp, h->gacc, h->gvel, ind_x, ind_y, h->sensor, force3);
+        if (h->gacc_q)
+            k_update_mixed<256><<<nb, 256, 0, h->stream>>>(h->dp, AccQ{h->gacc_q}, h->gvel, ind_x, ind_y, h->sensor,
+                                                           force3);
+        else
+            k_update_mixed<256><<<nb, 256, 0, h->stream>>>(h->dp, AccF4{h->gacc}, h->gvel, ind_x, ind_y, h->sensor,
+                                                           force3);
         CK_LAUNCH(h, "update mixed");
         return MPM_OK;
     }
@@ -329,8 +349,14 @@ int launch_update(mpm_handle* h, double ind_x, double ind_y, double* force3) {
 int launch_return_map_mixed(mpm_handle* h, int do_p2g) {
     const int cur = h->rm_parity;
     h->rm_parity ^= 1;
-    k_return_map_mixed<<<h->num_sms * 4, 128, 0, h->stream>>>(h->dp, mixed_state(h), h->rm_list, h->rm_counts + cur,
-                                                              h->rm_counts + (cur ^ 1), h->gacc, do_p2g, h->err);
+    if (h->gacc_q)
+        k_return_map_mixed<<<h->num_sms * 4, 128, 0, h->stream>>>(h->dp, mixed_state(h), h->rm_list,
+                                                                  h->rm_counts + cur, h->rm_counts + (cur ^ 1),
+                                                                  AccQ{h->gacc_q}, do_p2g, h->err);
+    else
+        k_return_map_mixed<<<h->num_sms * 4, 128, 0, h->stream>>>(h->dp, mixed_state(h), h->rm_list,
+                                                                  h->rm_counts + cur, h->rm_counts + (cur ^ 1),
+                                                                  AccF4{h->gacc}, do_p2g, h->err);
     CK_LAUNCH(h, "return map mixed");
     return MPM_OK;
 }
@@ -345,8 +371,14 @@ int launch_g2p2g_mixed(mpm_handle* h, int do_p2g, int record_pq, int store_vc) {
     int* const rm_count = h->rm_counts + h->rm_parity;
     // the warps' velocity boxes: kVBoxNodes float4 of dynamic shared memory per warp
     const size_t vsm = sizeof(float4) * (kFusedBlock / 32) * kVBoxNodes;
-    k_g2p2g_mixed<<<blocks_for(n, kFusedBlock), kFusedBlock, vsm, h->stream>>>(
-        h->dp, mixed_state(h), n, h->gvel, h->gacc, do_p2g, record_pq, store_vc, h->err, h->rm_list, rm_count);
+    if (h->gacc_q)
+        k_g2p2g_mixed<<<blocks_for(n, kFusedBlock), kFusedBlock, vsm, h->stream>>>(
+            h->dp, mixed_state(h), n, h->gvel, AccQ{h->gacc_q}, do_p2g, record_pq, store_vc, h->err, h->rm_list,
+            rm_count);
+    else
+        k_g2p2g_mixed<<<blocks_for(n, kFusedBlock), kFusedBlock, vsm, h->stream>>>(
+            h->dp, mixed_state(h), n, h->gvel, AccF4{h->gacc}, do_p2g, record_pq, store_vc, h->err, h->rm_list,
+            rm_count);
     CK_LAUNCH(h, "g2p2g mixed");
     return MPM_OK;
 }
@@ -369,7 +401,10 @@ int launch_g2p(mpm_handle* h, int record_pq) {
 
 int reset_grid(mpm_handle* h) {
     if (is_mixed(h)) {
-        CK(h, cudaMemsetAsync(h->gacc, 0, sizeof(float4) * (size_t)h->dp.nodes, h->stream));
+        if (h->gacc_q)
+            CK(h, cudaMemsetAsync(h->gacc_q, 0, sizeof(unsigned long long) * 4 * (size_t)h->dp.nodes, h->stream));
+        else
+            CK(h, cudaMemsetAsync(h->gacc, 0, sizeof(float4) * (size_t)h->dp.nodes, h->stream));
         h->p2g_ready = false;
         return MPM_OK;
     }
@@ -719,6 +754,21 @@ int mpm_sort(mpm_handle* h) {
     return r ? r : code;
 }
 
+int mpm_set_grid_accumulation(mpm_handle* h, int mode) {
+    if (!h || (mode != MPM_ACCUM_FLOAT && mode != MPM_ACCUM_FIXED)) return MPM_ERR_ARG;
+    if (!is_mixed(h)) return mode == MPM_ACCUM_FLOAT ? MPM_OK : MPM_ERR_ARG;
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (mode == MPM_ACCUM_FIXED && !h->gacc_q) {
+        CK(h, cudaMalloc(&h->gacc_q, sizeof(unsigned long long) * 4 * (size_t)h->dp.nodes));
+        CK(h, cudaMemsetAsync(h->gacc_q, 0, sizeof(unsigned long long) * 4 * (size_t)h->dp.nodes, h->stream));
+    } else if (mode == MPM_ACCUM_FLOAT && h->gacc_q) {
+        CK(h, cudaFree(h->gacc_q));
+        h->gacc_q = nullptr;
+    }
+    h->p2g_ready = false;   // the next step computes its P2G into the selected accumulator
+    return MPM_OK;
+}
+
 int mpm_set_sort_interval(mpm_handle* h, int k) {
     if (!h || k < 0) return MPM_ERR_ARG;
     h->sort_interval = k;
@@ -1020,7 +1070,7 @@ int mpm_set_partition(mpm_handle* h, int id, int x0, int gxp, unsigned id_base) 
 
 size_t mpm_halo_bytes(const mpm_handle* h) {
     if (!h) return 0;
-    return halo_nodes(h) * (is_mixed(h) ? sizeof(float4) : 4 * sizeof(double));
+    return halo_nodes(h) * (is_mixed(h) && !h->gacc_q ? sizeof(float4) : 4 * sizeof(double));
 }
 
 int mpm_halo_pack(mpm_handle* h, int side, void* dst) {
@@ -1029,7 +1079,11 @@ int mpm_halo_pack(mpm_handle* h, int side, void* dst) {
     if (!hn) return MPM_OK;
     const long long off = halo_offset(h, side);
     if (is_mixed(h)) {
-        CK(h, cudaMemcpyAsync(dst, h->gacc + off, sizeof(float4) * hn, cudaMemcpyDeviceToDevice, h->stream));
+        if (h->gacc_q)
+            CK(h, cudaMemcpyAsync(dst, h->gacc_q + 4 * off, sizeof(unsigned long long) * 4 * hn,
+                                  cudaMemcpyDeviceToDevice, h->stream));
+        else
+            CK(h, cudaMemcpyAsync(dst, h->gacc + off, sizeof(float4) * hn, cudaMemcpyDeviceToDevice, h->stream));
         return MPM_OK;
     }
     double* d = static_cast<double*>(dst);
@@ -1044,7 +1098,10 @@ int mpm_halo_add(mpm_handle* h, int side, const void* src) {
     const size_t hn = halo_nodes(h);
     if (!hn) return MPM_OK;
     const long long off = halo_offset(h, side);
-    if (is_mixed(h))
+    if (is_mixed(h) && h->gacc_q)
+        k_halo_add_q<<<blocks_for(4 * hn, 256), 256, 0, h->stream>>>(h->gacc_q, off, (int)hn,
+                                                                     static_cast<const unsigned long long*>(src));
+    else if (is_mixed(h))
         k_halo_add_f4<<<blocks_for(hn, 256), 256, 0, h->stream>>>(h->gacc, off, (int)hn,
                                                                   static_cast<const float4*>(src));
     else
@@ -1822,7 +1879,13 @@ int mpm_testing_active_nodes(mpm_handle* h, long long* count) {
     if (!h || !count) return MPM_ERR_ARG;
     const size_t nodes = (size_t)h->dp.nodes;
     long long c = 0;
-    if (is_mixed(h)) {
+    if (is_mixed(h) && h->gacc_q) {
+        std::vector<unsigned long long> g(4 * nodes);
+        CK(h, cudaMemcpyAsync(g.data(), h->gacc_q, sizeof(unsigned long long) * 4 * nodes, cudaMemcpyDeviceToHost,
+                              h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        for (size_t i = 0; i < nodes; i++) c += g[4 * i] != 0ull;
+    } else if (is_mixed(h)) {
         std::vector<float4> g(nodes);
         CK(h, cudaMemcpyAsync(g.data(), h->gacc, sizeof(float4) * nodes, cudaMemcpyDeviceToHost, h->stream));
         CK(h, cudaStreamSynchronize(h->stream));
@@ -1840,6 +1903,17 @@ int mpm_testing_active_nodes(mpm_handle* h, long long* count) {
 int mpm_testing_download_grid(mpm_handle* h, double* out, int which) {
     if (!h || !out) return MPM_ERR_ARG;
     const size_t nodes = (size_t)h->dp.nodes;
+    if (is_mixed(h) && h->gacc_q && !which) {
+        std::vector<unsigned long long> g(4 * nodes);
+        CK(h, cudaMemcpyAsync(g.data(), h->gacc_q, sizeof(unsigned long long) * 4 * nodes, cudaMemcpyDeviceToHost,
+                              h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        for (size_t i = 0; i < nodes; i++) {
+            out[i] = (double)(long long)g[4 * i] * h->dp.q_inv_m;
+            for (int c = 1; c < 4; c++) out[c * nodes + i] = (double)(long long)g[4 * i + c] * h->dp.q_inv_p;
+        }
+        return MPM_OK;
+    }
     if (is_mixed(h)) {
         std::vector<float4> g(nodes);
         CK(h, cudaMemcpyAsync(g.data(), which ? h->gvel : h->gacc, sizeof(float4) * nodes, cudaMemcpyDeviceToHost,

@@ -32,6 +32,14 @@ __global__ void k_halo_add_f4(float4* __restrict__ acc, long long off, int hn, c
     acc[off + i] = make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
 }
 
+// The same for the fixed-point accumulator (4 int64 per node): an exact sum.
+__global__ void k_halo_add_q(unsigned long long* __restrict__ acc, long long off, int hn,
+                             const unsigned long long* __restrict__ src) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 4 * hn) return;
+    acc[4 * off + i] += src[i];
+}
+
 // One particle record of a point transfer. FP64 handles: 32 doubles (the
 // 28 SoA rows, the apex shift p0, the upload id as bits, 2 unused); mixed
 // handles: 32 words (the 28 rows of the mixed state, p0 as a double in two

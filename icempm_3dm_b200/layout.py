@@ -22,6 +22,9 @@ PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 PRECISION_FP64_SVD64 = 2
 
+ACCUM_FLOAT = 0      # mixed P2G: FP32 float4 atomics (default)
+ACCUM_FIXED = 1      # mixed P2G: 64-bit fixed point, order-independent sums
+
 ERR_NAMES = {
     0: "ok", 5: "receive overflow",
     70: "particle outside grid (-x)", 71: "particle outside grid (-y)", 72: "particle outside grid (-z)",

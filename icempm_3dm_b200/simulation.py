@@ -86,6 +86,11 @@ class MPMHandle:
     def sort(self):
         return check(LIB.mpm_sort(self._h), "mpm_sort")
 
+    def set_grid_accumulation(self, mode):
+        """ACCUM_FLOAT (default) or ACCUM_FIXED (mixed handles: order-
+        independent fixed-point grid sums, runs repeat bit for bit)."""
+        check(LIB.mpm_set_grid_accumulation(self._h, int(mode)), "mpm_set_grid_accumulation")
+
     def upload_ids(self, ids):
         ids = np.ascontiguousarray(ids, dtype=np.uint32)
         check(LIB.mpm_upload_ids(self._h, uptr(ids), ids.size), "mpm_upload_ids")

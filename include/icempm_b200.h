@@ -143,6 +143,17 @@ int  mpm_download_cohesion(mpm_handle* h, double* cohesion, unsigned* n);
  * ProxyPoint3D::getCellIndex (proxypoint3d.cpp:158-163), stable (ties keep
  * their previous order). */
 int  mpm_sort(mpm_handle* h);
+/* New (no reference counterpart): the grid accumulator of the mixed P2G.
+ * MPM_ACCUM_FLOAT (default): float4 {m, m v} per node, FP32 vector atomics,
+ * whose rounding depends on the order of the adds. MPM_ACCUM_FIXED: each
+ * contribution in 64-bit fixed point (2^44 units per the larger particle
+ * mass, and per that mass at vmax for momentum), added as integers: the sums
+ * are exact and independent of the order, and a run repeats bit for bit in
+ * its particle state; 32 B per node instead of 16. FP64 handles accept only
+ * MPM_ACCUM_FLOAT (their FP64 sums are kept as they are). */
+#define MPM_ACCUM_FLOAT 0
+#define MPM_ACCUM_FIXED 1
+int  mpm_set_grid_accumulation(mpm_handle* h, int mode);
 /* Sort automatically every k substeps inside mpm_step (0 = never, the
  * default, as with one partition the reference never re-sorts). */
 int  mpm_set_sort_interval(mpm_handle* h, int k);
