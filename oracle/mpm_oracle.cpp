@@ -3,9 +3,9 @@
 // Restatement, in plain C++ with explicit 3x3 arithmetic (the reference uses
 // Eigen in device code), of the single-partition step of
 // simulation/mpm_kernels.cuh. Each function cites the lines it follows. The
-// parity status of this file is described in mpm_oracle.h: transfers and
-// constitutive model are unpinned against the reference itself (no golden
-// outputs exist, the reference cannot be built here), the SVD is pinned.
+// parity status of this file is described in mpm_oracle.h: the whole step is
+// pinned against the reference's own kernels compiled on the host, the SVD
+// bit for bit.
 //
 // The per-particle and per-node functions are templated on the scalar type:
 // double is the oracle proper; Dual (dual.h) runs the same arithmetic with a

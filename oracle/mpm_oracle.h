@@ -8,15 +8,16 @@
  * (icempm_3dm_b200/) links, imports or calls it.
  *
  * Parity pinning:
+ *   - the step (P2G, node update, G2P, the constitutive functions) is pinned
+ *     against the reference's own simulation/mpm_kernels.cuh, compiled
+ *     unmodified as host C++ from the reference tree (oracle/ref_kernels.cpp
+ *     over the Eigen-API stand-in of oracle/refshim/; oracle/Makefile target
+ *     `ref`): tests/test_oracle_vs_reference.py requires agreement to 1e-13
+ *     phase by phase and 1e-11 over 30 substeps on inputs that reach every
+ *     branch;
  *   - the 3x3 SVD restatement (or_svd3x3_f32) is pinned bit-for-bit against
- *     the reference's own helper_math.cuh svd<T>, compiled on the host from
- *     its source under the reference tree (oracle/Makefile target `ref`),
- *     and against golden vectors generated from it (tests/golden/svd_ref.npz);
- *   - the transfer and constitutive functions are PARITY UNPINNED against the
- *     reference itself: the reference ships no tests or golden outputs, and
- *     its kernels cannot be built here (Eigen3, HDF5-C++, spdlog, rapidjson
- *     and cxxopts are absent). They are pinned by known-answer tests
- *     (tests/test_oracle_physics.py) and follow the cited lines one to one.
+ *     the reference's own helper_math.cuh svd<T>, compiled the same way, and
+ *     against golden vectors generated from it (tests/golden/svd_ref.npz).
  *
  * Data layouts are the reference's:
  *   particles: host SoA, 28 rows of `pitch` doubles (parameters_sim_3d.h:29-38)

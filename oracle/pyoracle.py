@@ -1,9 +1,11 @@
 """CPU ORACLE — test infrastructure, not product code.
 
 ctypes bindings of oracle/liboracle.so (the C++ restatement of the
-reference step, see mpm_oracle.h) and of oracle/_ref/libref_svd.so (the
-reference's own helper_math.cuh SVD compiled on the host). Only tests/,
-__graft_entry__.smoke() and bench.py's cpu_baseline leg import this module.
+reference step, see mpm_oracle.h), of oracle/_ref/libref_svd.so (the
+reference's own helper_math.cuh SVD compiled on the host) and of
+oracle/_ref/libref_mpm.so (the reference's own mpm_kernels.cuh compiled on
+the host, driven by RefSim). Only tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline leg and reference arm import this module.
 """
 import ctypes
 import os

@@ -15,7 +15,8 @@ only in the order of rounded operations: Eigen's expression order against
 the oracle's explicit 3x3 arithmetic), 1e-12 for the recorded trial P and Q
 (J^2 - 1 near J = 1), 1e-11 for the indenter sensor bins (differences of
 nearly equal velocities); 30 substeps 1e-11 (the same
-rounding, carried through the run); integer status words bit for bit.
+rounding, carried through the run; C 1e-10, a difference quotient over h of
+node velocities); integer status words bit for bit.
 
 One reference behaviour is excluded from the comparison, on purpose: for
 liquid particles partition_kernel_g2p computes no trial p, q (ComputePQ runs
@@ -132,7 +133,8 @@ def test_thirty_substeps(name, prms, soa):
     assert rel(h_ref, h_or) < 1e-11
     assert np.array_equal(util_bits(ref.soa), util_bits(orc.soa))
     for fname, a, b in FIELDS:
-        assert rel(ref.soa[a:b], orc.soa[a:b]) < 1e-11, fname
+        # C = 4/h sum w v (x_i - x_p): node-velocity rounding scaled by 1/h
+        assert rel(ref.soa[a:b], orc.soa[a:b]) < (1e-10 if fname == "C" else 1e-11), fname
     assert ref.prms.SimulationStep == orc.prms.SimulationStep == 30
     assert ref.prms.indenter_x == orc.prms.indenter_x
 
