@@ -63,13 +63,15 @@ __device__ __forceinline__ float detm1(const float E[3][3]) {
     return tr + m2 + d;
 }
 
-// dev(F F^T) with F = I + E: dev(E + E^T + E E^T)
+// dev(F F^T) with F = I + E: dev(E + E^T + E E^T), symmetric (upper triangle mirrored)
 __device__ __forceinline__ void dev_b(const float E[3][3], float D[3][3]) {
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-        for (int j = 0; j < 3; j++)
+        for (int j = i; j < 3; j++) {
             D[i][j] = E[i][j] + E[j][i] + (E[i][0] * E[j][0] + E[i][1] * E[j][1] + E[i][2] * E[j][2]);
+            D[j][i] = D[i][j];
+        }
     const float t = (D[0][0] + D[1][1] + D[2][2]) * (1.0f / 3.0f);
     D[0][0] -= t; D[1][1] -= t; D[2][2] -= t;
 }
@@ -92,11 +94,8 @@ __device__ __forceinline__ ElasticInv elastic_invariants(const float E[3][3]) {
 
 __device__ __forceinline__ void trial_pq_inv(const DevParams& P, const ElasticInv& e, float& p_tr, float& q_tr) {
     p_tr = -P.f_hkappa * (e.jm1 * (e.J + 1.0f));
-    float sq = 0.f;
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) sq += e.D[i][j] * e.D[i][j];
+    const float off = e.D[0][1] * e.D[0][1] + e.D[0][2] * e.D[0][2] + e.D[1][2] * e.D[1][2];
+    const float sq = e.D[0][0] * e.D[0][0] + e.D[1][1] * e.D[1][1] + e.D[2][2] * e.D[2][2] + 2.0f * off;
     q_tr = P.f_qmu * e.jm23 * sqrtf(sq);
 }
 
@@ -263,7 +262,8 @@ __device__ __forceinline__ void g2p_gather_staged(const DevParams& P, const floa
     if (part && staged) {
         // v = sum w nv and the first moments M_k = sum w nv o_k over the node
         // offsets o = (a, b, c); C = 4/h sum w nv (o - f) = 4/h (M - f v)
-        // (mpm_kernels.cuh:278-305 summed in this order).
+        // (mpm_kernels.cuh:278-305). The weights factor, w = wx_a wy_b wz_c, so
+        // each stencil row first sums T = sum_c wz_c nv and Z = sum_c c wz_c nv.
         float ww[3][3];
         quad_weights<float>(fx, ww);
         wx.put(ww);
@@ -271,39 +271,43 @@ __device__ __forceinline__ void g2p_gather_staged(const DevParams& P, const floa
 #pragma unroll
         for (int r = 0; r < 3; r++) { v[r] = 0.f; Mx[r] = 0.f; My[r] = 0.f; Mz[r] = 0.f; }
         const int t0 = ((base[0] - lo0) * ey + (base[1] - lo1)) * ez + (base[2] - lo2);
+        const float wz0 = ww[0][2], wz1 = ww[1][2], wz2 = ww[2][2], wz2d = 2.0f * ww[2][2];
 #pragma unroll 1
         for (int a = 0; a < 3; a++) {
             const float wa = wx.get(a);
-            float ra[3] = {0.f, 0.f, 0.f};
+            float ra[3];
 #pragma unroll
             for (int b = 0; b < 3; b++) {
                 const float wab = wa * ww[b][1];
+                const float bwab = (float)b * wab;
                 const float4* row = vbox + (t0 + a * ey * ez + b * ez);
-                float rb[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    const float4 nd = row[c];
-                    const float w = wab * ww[c][2];
-                    const float wn[3] = {w * nd.x, w * nd.y, w * nd.z};
-#pragma unroll
-                    for (int r = 0; r < 3; r++) {
-                        rb[r] += wn[r];
-                        if (c == 1) Mz[r] += wn[r];
-                        if (c == 2) Mz[r] += 2.0f * wn[r];
-                    }
+                float T[3], Z[3];
+                {
+                    const float4 nd = row[0];
+                    T[0] = wz0 * nd.x; T[1] = wz0 * nd.y; T[2] = wz0 * nd.z;
+                }
+                {
+                    const float4 nd = row[1];
+                    T[0] = fmaf(wz1, nd.x, T[0]); T[1] = fmaf(wz1, nd.y, T[1]); T[2] = fmaf(wz1, nd.z, T[2]);
+                    Z[0] = wz1 * nd.x; Z[1] = wz1 * nd.y; Z[2] = wz1 * nd.z;
+                }
+                {
+                    const float4 nd = row[2];
+                    T[0] = fmaf(wz2, nd.x, T[0]); T[1] = fmaf(wz2, nd.y, T[1]); T[2] = fmaf(wz2, nd.z, T[2]);
+                    Z[0] = fmaf(wz2d, nd.x, Z[0]); Z[1] = fmaf(wz2d, nd.y, Z[1]); Z[2] = fmaf(wz2d, nd.z, Z[2]);
                 }
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
-                    ra[r] += rb[r];
-                    if (b == 1) My[r] += rb[r];
-                    if (b == 2) My[r] += 2.0f * rb[r];
+                    ra[r] = b == 0 ? wab * T[r] : fmaf(wab, T[r], ra[r]);
+                    if (b > 0) My[r] = fmaf(bwab, T[r], My[r]);
+                    Mz[r] = fmaf(wab, Z[r], Mz[r]);
                 }
             }
             const float fa = (float)a;
 #pragma unroll
             for (int r = 0; r < 3; r++) {
                 v[r] += ra[r];
-                Mx[r] += fa * ra[r];
+                Mx[r] = fmaf(fa, ra[r], Mx[r]);
             }
         }
         const float s4 = P.f_s4;
