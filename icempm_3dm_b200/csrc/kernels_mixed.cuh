@@ -221,8 +221,8 @@ __device__ __forceinline__ void g2p_gather_mixed(const DevParams& P, const float
 
 // Gather with the warp's velocity box staged in shared memory. The warp's
 // lanes with an in-grid stencil (part) span a box of base cells; the box's
-// nodes (base .. base+2 per axis) are read from the grid once, row by row
-// along z (coalesced), into this warp's slice vbox[VCAP], and each lane then
+// nodes (base .. base+2 per axis) are copied from the grid once, row by row
+// along z (coalesced, 16-byte cp.async), into this warp's slice vbox[VCAP], and each lane then
 // gathers its 27 nodes from shared memory. A box larger than VCAP, or lanes
 // whose stencil leaves the grid, take the global gather. Called by the whole
 // warp (the box, the loads and __syncwarp are warp-wide).
@@ -254,8 +254,13 @@ __device__ __forceinline__ void g2p_gather_staged(const DevParams& P, const floa
                 const int tz = k - row * ez;
                 const int tx = (int)(((float)row + 0.5f) * inv_ey);
                 const int ty = row - tx * ey;
-                vbox[k] = __ldg(vel + (g0 + tx * slab + ty * gz + tz));
+                // global -> shared without a round trip through registers: the
+                // lane issues all its copies before it waits for any of them
+                const unsigned dst = (unsigned)__cvta_generic_to_shared(vbox + k);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 16;"
+                             :: "r"(dst), "l"(vel + (g0 + tx * slab + ty * gz + tz)) : "memory");
             }
+            asm volatile("cp.async.wait_all;" ::: "memory");
             __syncwarp();
         }
     }
