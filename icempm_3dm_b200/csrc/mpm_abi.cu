@@ -330,11 +330,12 @@ int launch_update(mpm_handle* h, double ind_x, double ind_y, double* force3) {
     // the nodes of the partition's window (one partition: the whole grid)
     const unsigned nb = blocks_for((long long)h->dp.node_hi - h->dp.node_lo, 256);
     if (is_mixed(h)) {
+        const unsigned nbm = blocks_for((long long)h->dp.node_hi - h->dp.node_lo, 256 * kUpdateNodesPerThread);
         if (h->gacc_q)
-            k_update_mixed<256><<<nb, 256, 0, h->stream>>>(h->dp, AccQ{h->gacc_q}, h->gvel, ind_x, ind_y, h->sensor,
+            k_update_mixed<256><<<nbm, 256, 0, h->stream>>>(h->dp, AccQ{h->gacc_q}, h->gvel, ind_x, ind_y, h->sensor,
                                                            force3);
         else
-            k_update_mixed<256><<<nb, 256, 0, h->stream>>>(h->dp, AccF4{h->gacc}, h->gvel, ind_x, ind_y, h->sensor,
+            k_update_mixed<256><<<nbm, 256, 0, h->stream>>>(h->dp, AccF4{h->gacc}, h->gvel, ind_x, ind_y, h->sensor,
                                                            force3);
         CK_LAUNCH(h, "update mixed");
         return MPM_OK;
