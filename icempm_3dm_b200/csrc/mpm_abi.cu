@@ -315,9 +315,9 @@ int launch_p2g(mpm_handle* h) {
     if (n == 0) return MPM_OK;
     if (is_mixed(h)) {
         if (h->gacc_q)
-            k_p2g_mixed<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->dp, mixed_state(h), n, AccQ{h->gacc_q}, h->err);
+            k_p2g_mixed<<<blocks_for(n, 128), 128, 0, h->stream>>>(h->dp, mixed_state(h), n, AccQ{h->gacc_q}, h->err);
         else
-            k_p2g_mixed<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->dp, mixed_state(h), n, AccF4{h->gacc}, h->err);
+            k_p2g_mixed<<<blocks_for(n, 128), 128, 0, h->stream>>>(h->dp, mixed_state(h), n, AccF4{h->gacc}, h->err);
         CK_LAUNCH(h, "p2g mixed");
         return MPM_OK;
     }
