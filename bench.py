@@ -15,6 +15,9 @@ host buffers (pinned SoA and cohesion uploaded, the cell-key sort, K substeps
 with the force history read back, SoA downloaded) inside the timed region. N > 1 runs independent
 replicas, one per GPU (the path is one partition; no collective).
 
+--partitions N times N x-slab partitions (the in-process driver) against
+one partition of the same driver on the same block (--halo slabs).
+
 --impl reference times the reference's own step kernels (mpm_kernels.cuh
 compiled as host C++ from its source into oracle/_ref, OpenMP on all host
 cores; the oracle port when that build is absent), without loading the
@@ -61,6 +64,11 @@ def parse():
     ap.add_argument("--adjoint", action="store_true",
                     help="time the adjoint (forward with checkpoints + reverse sweep) on the calibration workload")
     ap.add_argument("--ckpt-every", type=int, default=20)
+    ap.add_argument("--partitions", type=int, default=0,
+                    help="time N x-slab partitions in this process (mpm_multi_*, on --gpus devices) "
+                         "against one partition of the same driver on the same block")
+    ap.add_argument("--halo", type=int, default=15,
+                    help="GridHaloSize of the --partitions run (the reference's default is 15)")
     return ap.parse_args()
 
 
@@ -533,12 +541,67 @@ def run_adjoint(args):
     return 0
 
 
+def run_partitions(args):
+    """One JSON line: the x-slab partitions of the reference's multi-partition
+    GPU_Implementation6 (the in-process driver mpm_multi_*: halo exchange after
+    every P2G, point transfers, the transfer-frequency rule and rebalance) with
+    --partitions partitions, against the same driver with one partition, on
+    the same block (GridHaloSize --halo). Partition i runs on device i % --gpus
+    (not under torchrun: one process drives all devices). Wall clock around
+    --steps substeps after --warmup; each call ends with the force history
+    read back, so the clock covers all device work and the driver's own host
+    time."""
+    import dataclasses
+    import torch
+    from icempm_3dm_b200 import PRECISION_FP64, PRECISION_MIXED
+    from icempm_3dm_b200 import generator as gen
+    from icempm_3dm_b200.partitions import PartitionedSim
+    prec = PRECISION_MIXED if args.precision == "mixed" else PRECISION_FP64
+    cfg = dataclasses.replace(gen.CONFIGS[args.workload], halo=args.halo)
+    prms, soa, coh = gen.make_block(cfg)
+    n = soa.shape[1]
+    devices = tuple(range(max(args.gpus, 1)))
+    runs = {}
+    for nparts in (1, args.partitions):
+        p = prms.copy()
+        p.nPartitions = nparts
+        with PartitionedSim(p, n, prec, devices=devices) as m:
+            m.upload(soa, cohesion=coh)
+            m.step(max(args.warmup, 3))
+            for d in devices:
+                torch.cuda.synchronize(d)
+            t0 = time.perf_counter()
+            hist = m.step(args.steps)
+            for d in devices:
+                torch.cuda.synchronize(d)
+            ms = (time.perf_counter() - t0) * 1e3
+            most, rebalances, ptf = m.stats()
+            moved = sum(nd for _, _, _, nd in m.info())
+        runs[nparts] = {"value": n * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps,
+                        "points_moved": moved, "largest_transfer": most, "rebalances": rebalances,
+                        "point_transfer_frequency": ptf, "force_norm": float(np.linalg.norm(hist))}
+    one, many = runs[1], runs[args.partitions]
+    out = {"metric": "particle-steps/s", "value": many["value"], "unit": "particle-steps/s",
+           "n_gpus": len(devices), "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": many["ms_per_step"], "higher_is_better": True, "scaling": "strong",
+           "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+           "config": {"workload": args.workload, "particles": n, "precision": args.precision,
+                      "partitions": args.partitions, "devices": list(devices), "halo": args.halo,
+                      "timing": "wall clock around mpm_multi_step"},
+           "one_partition": one, "partitioned": many,
+           "partitioned_over_one": many["value"] / one["value"]}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.adjoint:
         return run_adjoint(args)
+    if args.partitions:
+        return run_partitions(args)
     return run_ours(args)
 
 

@@ -208,3 +208,20 @@ def test_one_partition_per_process_matches(precision, tmp_path):
     assert sum(int(p["moved"]) for p in parts) > 0
     compare(f"{world} processes ({'fp64' if precision == PRECISION_FP64 else 'mixed'})", parts[0]["hist"],
             by_id(out, ids, n), ref_hist, ref_full, precision == PRECISION_FP64)
+
+
+def test_bench_partitions_line():
+    """bench.py --partitions: one JSON line with the partitioned and the
+    one-partition run of the same driver; the FP64 force histories agree."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--workload", "block250k", "--precision",
+                        "fp64", "--partitions", "3", "--steps", "20", "--warmup", "3"],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
+    assert line["config"]["partitions"] == 3 and line["value"] > 0
+    one, many = line["one_partition"]["force_norm"], line["partitioned"]["force_norm"]
+    assert one > 0 and abs(many - one) <= 1e-9 * one
