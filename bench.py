@@ -15,6 +15,9 @@ host buffers (pinned SoA and cohesion uploaded, the cell-key sort, K substeps
 with the force history read back, SoA downloaded) inside the timed region. N > 1 runs independent
 replicas, one per GPU (the path is one partition; no collective).
 
+--io times the IO around the step (frame records, snapshot write/read,
+download/upload).
+
 --partitions N times N x-slab partitions (the in-process driver) against
 one partition of the same driver on the same block (--halo slabs).
 
@@ -67,6 +70,9 @@ def parse():
     ap.add_argument("--partitions", type=int, default=0,
                     help="time N x-slab partitions in this process (mpm_multi_*, on --gpus devices) "
                          "against one partition of the same driver on the same block")
+    ap.add_argument("--io", action="store_true",
+                    help="time the IO around the step: animation-frame records, SoA download, snapshot "
+                         "write and read, upload")
     ap.add_argument("--halo", type=int, default=15,
                     help="GridHaloSize of the --partitions run (the reference's default is 15)")
     return ap.parse_args()
@@ -594,8 +600,115 @@ def run_partitions(args):
     return 0
 
 
+def run_io(args):
+    """One JSON line: the IO of the reference's SnapshotManager and
+    transfer_from_device around the step, on the block after --warmup
+    substeps, each by wall clock (seconds):
+      - frame_full / frame_partial: mpm_frame_records, the records of a full
+        animation frame (VisualPoint per point) and of a partial frame 1,000
+        substeps later (UpdatePos / UpdateJp / UpdateStatus), built on the
+        device and copied into preallocated host arrays;
+      - save_frame_full / save_frame_partial: v%05d.h5 written by the HDF5
+        codec (deflate 5, as the reference; chunks compressed on a thread
+        pool);
+      - download: mpm_download_soa of the 28-row FP64 SoA;
+      - save_snapshot / read_snapshot: d%05d.h5, uncompressed;
+      - upload: mpm_upload_soa + mpm_upload_cohesion of the SoA read back.
+    cpu_baseline: the float32 CPU restatement of the frame-record logic
+    (oracle/frames.py, numpy) on the downloaded SoA, full and partial."""
+    import ctypes
+    import shutil
+    import tempfile
+    import torch
+    from icempm_3dm_b200 import MPMHandle, PRECISION_FP64, PRECISION_MIXED
+    from icempm_3dm_b200 import generator as gen
+    from icempm_3dm_b200 import snapshot as snap
+    from icempm_3dm_b200._lib import LIB, check
+    torch.cuda.set_device(0)
+    prec = PRECISION_MIXED if args.precision == "mixed" else PRECISION_FP64
+    cfg = gen.CONFIGS[args.workload]
+    prms, soa, coh = gen.make_block(cfg)
+    n = soa.shape[1]
+    h = MPMHandle(prms, n, prec)
+    h.upload(soa, cohesion=coh)
+    h.sort()
+    h.step(max(args.warmup, 3))
+    t = {}
+
+    def clock(name, fn):
+        t0 = time.perf_counter()
+        r = fn()
+        t[name] = time.perf_counter() - t0
+        return r
+
+    pts = np.zeros(n, dtype=snap.VISUAL_POINT)
+    pv, jp, st = (np.zeros(n, dtype=d) for d in (snap.UPDATE_POS, snap.UPDATE_JP, snap.UPDATE_STATUS))
+    cnt = [ctypes.c_uint(0) for _ in range(4)]
+
+    def full_records(frame):
+        check(LIB.mpm_frame_records(h._h, frame, 1, pts.ctypes.data, ctypes.byref(cnt[0]), None, None, None, None,
+                                    None, None), "mpm_frame_records")
+
+    def partial_records(frame):
+        check(LIB.mpm_frame_records(h._h, frame, 0, None, None, pv.ctypes.data, ctypes.byref(cnt[1]),
+                                    jp.ctypes.data, ctypes.byref(cnt[2]), st.ctypes.data, ctypes.byref(cnt[3])),
+              "mpm_frame_records")
+
+    full_records(0)                                  # first call: the library's frame buffers
+    clock("frame_full", lambda: full_records(1))
+    n_full = cnt[0].value
+    h.step(1000)
+    clock("frame_partial", lambda: partial_records(2))
+    n_part = [c.value for c in cnt[1:]]
+    sens, force = h.sensors()
+    out_dir = tempfile.mkdtemp(prefix="icempm_io_")
+    try:
+        p = h.params()
+        f_full = clock("save_frame_full", lambda: snap.save_frame(out_dir, 1, p, sens, force, False,
+                                                                 points=pts[:n_full]))
+        f_part = clock("save_frame_partial", lambda: snap.save_frame(
+            out_dir, 2, p, sens, force, True, upd_pos=pv[:n_part[0]], upd_jp=jp[:n_part[1]],
+            upd_status=st[:n_part[2]]))
+        down = clock("download", lambda: h.download())
+        m = down.shape[1]
+        buf = np.zeros((28, n))
+        buf[:, :m] = down
+        f_snap = clock("save_snapshot", lambda: snap.save_snapshot(out_dir, 3, p, buf, m, sens, compress=False))
+        _, back, size, _ = clock("read_snapshot", lambda: snap.read_snapshot(f_snap))
+        c = h.cohesion()
+        clock("upload", lambda: h.upload(np.ascontiguousarray(back[:, :size]), cohesion=c))
+        sizes = {k: os.path.getsize(v) for k, v in (("frame_full", f_full), ("frame_partial", f_part),
+                                                    ("snapshot", f_snap))}
+    finally:
+        shutil.rmtree(out_dir, ignore_errors=True)
+    # the CPU restatement of the record logic on the same points
+    from oracle.frames import FrameState
+    fs = FrameState()
+    t0 = time.perf_counter()
+    fs.full(down, 1)
+    cpu_full = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    fs.partial(down, 2, p.InitialTimeStep, p.UpdateEveryNthStep, p.animation_threshold_pos)
+    cpu_part = time.perf_counter() - t0
+    rec_bytes = {"frame_full": n_full * snap.VISUAL_POINT.itemsize,
+                 "frame_partial": n_part[0] * snap.UPDATE_POS.itemsize + n_part[1] * snap.UPDATE_JP.itemsize
+                 + n_part[2] * snap.UPDATE_STATUS.itemsize, "soa": 28 * 8 * m}
+    out = {"metric": "seconds", "value": t["frame_full"], "unit": "s", "n_gpus": 1, "higher_is_better": False,
+           "data": "synthetic", "dtype": args.precision,
+           "config": {"workload": args.workload, "particles": n, "precision": args.precision},
+           "seconds": t, "records": {"full": n_full, "partial_pos": n_part[0], "partial_jp": n_part[1],
+                                     "partial_status": n_part[2]},
+           "bytes": rec_bytes, "file_bytes": sizes,
+           "cpu_baseline": {"frame_full": cpu_full, "frame_partial": cpu_part, "unit": "s", "cores": 1,
+                            "kind": "port", "sample": f"the {m} downloaded points (numpy)"}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.io:
+        return run_io(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.adjoint:

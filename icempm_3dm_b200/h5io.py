@@ -28,6 +28,7 @@ import mmap
 import os
 import struct
 import zlib
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -565,16 +566,31 @@ class H5Writer:
                 raise H5Error("chunk shape must have the dataset's rank")
             entries = []
             grid = [range(0, s, c) for s, c in zip(shape, chunks)]
-            for off in np.ndindex(*[len(g) for g in grid]):
-                o = tuple(g[i] for g, i in zip(grid, off))
+            offs = [tuple(g[i] for g, i in zip(grid, off)) for off in np.ndindex(*[len(g) for g in grid])]
+
+            def encode(o):
                 block = np.zeros(chunks, dtype=data.dtype)
                 src = tuple(slice(a, min(a + c, s)) for a, c, s in zip(o, chunks, shape))
                 block[tuple(slice(0, x.stop - x.start) for x in src)] = data[src]
                 raw = block.tobytes()
-                if deflate is not None:
-                    raw = zlib.compress(raw, int(deflate))
-                entries.append((o, len(raw), self._tell()))
-                self._f.write(raw)
+                return zlib.compress(raw, int(deflate)) if deflate is not None else raw
+
+            # zlib releases the GIL: deflated chunks are compressed on a pool
+            # of threads, a window at a time, and written in chunk order (the
+            # file's bytes do not depend on the number of threads)
+            workers = min(len(offs), os.cpu_count() or 1, 32) if deflate is not None else 1
+            if workers > 1:
+                with ThreadPoolExecutor(workers) as ex:
+                    for i in range(0, len(offs), 2 * workers):
+                        window = offs[i:i + 2 * workers]
+                        for o, raw in zip(window, ex.map(encode, window)):
+                            entries.append((o, len(raw), self._tell()))
+                            self._f.write(raw)
+            else:
+                for o in offs:
+                    raw = encode(o)
+                    entries.append((o, len(raw), self._tell()))
+                    self._f.write(raw)
             layout = ("chunked", entries, chunks)
         self._sets.append((name, shape, data.dtype, layout, deflate, list((attrs or {}).items())))
 

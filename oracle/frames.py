@@ -12,7 +12,7 @@ changes.
 """
 import numpy as np
 
-from icempm_3dm_b200._lib import IDX_JP_INV, IDX_UTILITY, POSX, VELX
+from icempm_3dm_b200.layout import IDX_JP_INV, IDX_UTILITY, POSX, VELX
 
 STATUS_CRUSHED, STATUS_DISABLED = 0x10000, 0x20000
 THRESHOLD_JP = np.float32(1e-2)
