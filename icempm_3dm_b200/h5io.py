@@ -258,19 +258,33 @@ class H5File:
         cshape = tuple(cdims[:rank])
         out = np.zeros(shape, dtype=dt)
         cbytes = int(np.prod(cshape)) * dt.itemsize
+        chunks = []
         for off, size, mask, addr in self._chunks(btree, rank):
             a = self._a(addr)
             self._check(a, size)
             if any(o >= s for o, s in zip(off, shape)):
                 raise H5Error(f"{name}: chunk offset {off} outside the dataspace {shape}")
-            raw = bytes(self._b[a:a + size])
-            raw = _unfilter(raw, filters, mask, dt.itemsize)
+            chunks.append((off, a, size, mask))
+
+        def decode(item):
+            off, a, size, mask = item
+            raw = _unfilter(bytes(self._b[a:a + size]), filters, mask, dt.itemsize)
             if len(raw) != cbytes:
                 raise H5Error(f"{name}: chunk at {off} decodes to {len(raw)} bytes, expected {cbytes}")
             chunk = np.frombuffer(raw, dtype=dt).reshape(cshape)
             dst = tuple(slice(o, min(o + c, s)) for o, c, s in zip(off, cshape, shape))
             src = tuple(slice(0, d.stop - d.start) for d in dst)
             out[dst] = chunk[src]
+
+        # filtered chunks decode on a pool of threads (zlib releases the GIL);
+        # each writes its own part of out
+        workers = min(len(chunks), os.cpu_count() or 1, 32) if filters else 1
+        if workers > 1:
+            with ThreadPoolExecutor(workers) as ex:
+                list(ex.map(decode, chunks))
+        else:
+            for item in chunks:
+                decode(item)
         return out
 
     def _chunks(self, btree, rank):

@@ -168,3 +168,26 @@ def test_writer_rejects_names_outside_the_root_group(tmp_path):
     with pytest.raises(h5io.H5Error):
         with h5io.H5Writer(tmp_path / "n.h5") as w:
             w.create_dataset("a/b", np.zeros(3))
+
+
+def test_deflated_chunks_do_not_depend_on_the_thread_count(tmp_path, monkeypatch):
+    """Chunks are compressed and decoded on a pool of threads: the file's bytes
+    are those of a one-thread write, and the data reads back exactly."""
+    rng = np.random.default_rng(7)
+    data = rng.standard_normal((37, 5000)).astype(np.float32)
+    data[:, ::3] = 0.0                                   # something for deflate to find
+
+    def write(path):
+        with h5io.H5Writer(path) as w:
+            w.create_dataset("A", data, chunks=(8, 1024), deflate=5)
+            w.create_dataset("B", data.reshape(-1)[:70001], chunks=(4096,), deflate=1)
+        return path.read_bytes()
+
+    many = write(tmp_path / "many.h5")
+    monkeypatch.setattr(os, "cpu_count", lambda: 1)
+    one = write(tmp_path / "one.h5")
+    assert many == one
+    monkeypatch.undo()
+    with h5io.H5File(tmp_path / "many.h5") as f:
+        assert np.array_equal(f.read("A"), data)
+        assert np.array_equal(f.read("B"), data.reshape(-1)[:70001])
