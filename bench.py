@@ -611,7 +611,9 @@ def run_io(args):
       - save_frame_full / save_frame_partial: v%05d.h5 written by the HDF5
         codec (deflate 5, as the reference; chunks compressed on a thread
         pool);
-      - download: mpm_download_soa of the 28-row FP64 SoA;
+      - download: mpm_download_soa of the 28-row FP64 SoA into a new array;
+        download_pinned / upload_pinned: the same into and out of page-locked
+        memory (pinned_empty, as the reference's HostSideSOA buffer);
       - save_snapshot / read_snapshot: d%05d.h5, uncompressed;
       - upload: mpm_upload_soa + mpm_upload_cohesion of the SoA read back.
     cpu_baseline: the float32 CPU restatement of the frame-record logic
@@ -620,7 +622,7 @@ def run_io(args):
     import shutil
     import tempfile
     import torch
-    from icempm_3dm_b200 import MPMHandle, PRECISION_FP64, PRECISION_MIXED
+    from icempm_3dm_b200 import MPMHandle, PRECISION_FP64, PRECISION_MIXED, pinned_empty
     from icempm_3dm_b200 import generator as gen
     from icempm_3dm_b200 import snapshot as snap
     from icempm_3dm_b200._lib import LIB, check
@@ -671,12 +673,18 @@ def run_io(args):
             upd_status=st[:n_part[2]]))
         down = clock("download", lambda: h.download())
         m = down.shape[1]
+        host = pinned_empty((28, n))
+        h.download(out=host)                         # first touch of the pages
+        clock("download_pinned", lambda: h.download(out=host))
         buf = np.zeros((28, n))
         buf[:, :m] = down
         f_snap = clock("save_snapshot", lambda: snap.save_snapshot(out_dir, 3, p, buf, m, sens, compress=False))
         _, back, size, _ = clock("read_snapshot", lambda: snap.read_snapshot(f_snap))
         c = h.cohesion()
         clock("upload", lambda: h.upload(np.ascontiguousarray(back[:, :size]), cohesion=c))
+        host[:, :size] = back[:, :size]
+        clock("upload_pinned", lambda: h.upload(host[:, :size] if size == n else
+                                                 np.ascontiguousarray(host[:, :size]), cohesion=c))
         sizes = {k: os.path.getsize(v) for k, v in (("frame_full", f_full), ("frame_partial", f_part),
                                                     ("snapshot", f_snap))}
     finally:

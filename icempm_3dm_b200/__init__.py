@@ -16,7 +16,7 @@ _EXPORTS = {
     "PRECISION_FP64_SVD64": "layout", "N_PTS_ARRAYS": "layout",
     "LIB": "_lib", "LIB_PATH": "_lib", "MPMError": "_lib",
     "MPMHandle": "simulation", "GPU_Implementation6": "simulation", "Model3D": "simulation",
-    "SnapshotManager": "simulation",
+    "SnapshotManager": "simulation", "pinned_empty": "simulation",
 }
 
 __all__ = sorted(_EXPORTS)

@@ -57,6 +57,8 @@ ENTRY_POINTS = [
     ("mpm_get_params", ctypes.c_int, [_hp, _pp]),
     ("mpm_count", ctypes.c_int, [_hp, _up]),
     ("mpm_last_error_string", ctypes.c_char_p, []),
+    ("mpm_host_alloc", ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]),
+    ("mpm_host_free", ctypes.c_int, [ctypes.c_void_p]),
     ("mpm_adjoint_forward", ctypes.c_int, [_hp, ctypes.c_int, ctypes.c_int, _dp]),
     ("mpm_adjoint_backward", ctypes.c_int, [_hp, _dp, _dp, _dp]),
     ("mpm_adjoint_state", ctypes.c_int, [_hp, _dp, ctypes.c_uint]),

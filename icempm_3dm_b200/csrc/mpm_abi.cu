@@ -1021,6 +1021,24 @@ int mpm_count(mpm_handle* h, unsigned* n) {
 
 const char* mpm_last_error_string(void) { return g_last_error; }
 
+int mpm_host_alloc(size_t bytes, void** ptr) {
+    if (!ptr) return MPM_ERR_ARG;
+    *ptr = nullptr;
+    if (bytes == 0) return MPM_OK;
+    const cudaError_t e = cudaMallocHost(ptr, bytes);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        return cuda_fail(nullptr, e, "cudaMallocHost");
+    }
+    return MPM_OK;
+}
+
+int mpm_host_free(void* ptr) {
+    if (!ptr) return MPM_OK;
+    const cudaError_t e = cudaFreeHost(ptr);
+    return e == cudaSuccess ? MPM_OK : cuda_fail(nullptr, e, "cudaFreeHost");
+}
+
 }  // extern "C"
 
 // ------------------------------------------------- x-slab partitions

@@ -67,9 +67,20 @@ class MPMHandle:
         check(LIB.mpm_count(self._h, ctypes.byref(n)), "mpm_count")
         return n.value
 
-    def download(self, raise_on_error=True):
+    def download(self, raise_on_error=True, out=None):
+        """mpm_download_soa: the particles as a (28, n) SoA. out: a
+        C-contiguous float64 array of 28 rows and at least n columns (e.g.
+        from pinned_empty, which copies at the host link's speed) that
+        receives them; the view out[:, :n] is returned."""
         n = self.count()
-        soa = np.zeros((N_PTS_ARRAYS, max(n, 1)), dtype=np.float64)
+        if out is None:
+            soa = np.zeros((N_PTS_ARRAYS, max(n, 1)), dtype=np.float64)
+        else:
+            if (out.dtype != np.float64 or out.ndim != 2 or out.shape[0] != N_PTS_ARRAYS
+                    or not out.flags.c_contiguous or out.shape[1] < max(n, 1)):
+                raise ValueError(f"out must be a C-contiguous float64 array of {N_PTS_ARRAYS} rows and at least "
+                                 f"{max(n, 1)} columns")
+            soa = out
         nn = ctypes.c_uint(0)
         code = LIB.mpm_download_soa(self._h, dptr(soa), soa.shape[1], ctypes.byref(nn))
         if raise_on_error:
@@ -254,8 +265,31 @@ class MPMHandle:
         return adj[:, :n]
 
 
+def pinned_empty(shape, dtype=np.float64):
+    """An uninitialised array over page-locked host memory (mpm_host_alloc,
+    the memory HostSideSOA::Allocate takes, host_side_soa.cpp:70-86): copies
+    between it and the device run at the host link's speed. The memory is
+    released (mpm_host_free) when the last array over it is gone."""
+    dtype = np.dtype(dtype)
+    nbytes = int(np.prod(shape)) * dtype.itemsize
+    if nbytes == 0:
+        return np.empty(shape, dtype=dtype)
+    ptr = ctypes.c_void_p()
+    check(LIB.mpm_host_alloc(nbytes, ctypes.byref(ptr)), "mpm_host_alloc")
+
+    class PinnedBytes(ctypes.c_char * nbytes):
+        def __del__(self):
+            LIB.mpm_host_free(ctypes.c_void_p(ctypes.addressof(self)))
+
+    return np.frombuffer(PinnedBytes.from_address(ptr.value), dtype=dtype).reshape(shape)
+
+
 class GPU_Implementation6:
-    """Method-for-method mirror of the reference class for one partition."""
+    """Method-for-method mirror of the reference class for one partition.
+    transfer_from_device downloads into one page-locked host buffer of the
+    handle's capacity, reused from frame to frame as the reference reuses
+    HostSideSOA's buffer: hssoa is a view of it, overwritten by the next
+    transfer."""
 
     def __init__(self, prms, precision=PRECISION_FP64, device=0):
         self.prms = prms
@@ -265,6 +299,7 @@ class GPU_Implementation6:
         self.hssoa = None
         self.indenter_force = np.zeros(3)
         self.indenter_sensor_total = None
+        self._host = None
 
     # GPU_Implementation6::initialize (gpu_implementation6.cpp:319-337), allocate_arrays (:385-401),
     # update_constants (:522-525)
@@ -309,7 +344,10 @@ class GPU_Implementation6:
         self.handle.reset_indenter_force_accumulator()
 
     def transfer_from_device(self):
-        self.hssoa = self.handle.download()
+        cap = max(self.handle.capacity, 1)
+        if self._host is None or self._host.shape[1] < cap:
+            self._host = pinned_empty((N_PTS_ARRAYS, cap))
+        self.hssoa = self.handle.download(out=self._host)
         sensor, total = self.handle.sensors()
         self.indenter_sensor_total = sensor
         self.indenter_force = total

@@ -112,6 +112,15 @@ int  mpm_update_constants(mpm_handle* h, const SimParams3D* prms);
 
 /* -------------------------------------------------------- particle data */
 
+/* HostSideSOA::Allocate (host_side_soa.cpp:70-86) allocates the host SoA as
+ * page-locked memory (cudaMallocHost), so that the uploads and downloads of
+ * the SoA run at the host link's speed. mpm_host_alloc gives such memory to
+ * a host that does not link CUDA itself: *ptr receives bytes of page-locked
+ * host memory (NULL for bytes == 0). Release it with mpm_host_free, as the
+ * reference does with cudaFreeHost (host_side_soa.cpp:72). */
+int  mpm_host_alloc(size_t bytes, void** ptr);
+int  mpm_host_free(void* ptr);
+
 /* GPU_Implementation6::transfer_ponts_to_device (gpu_implementation6.cpp:404-414),
  * GPU_Partition_3D::transfer_points_from_soa_to_device (gpu_partition_3d.cu:201-215):
  * n particles from a host SoA in the reference's HostSideSOA row layout

@@ -5,7 +5,7 @@
  *
  *   HostSideSOA          the pinned-buffer SoA of host_side_soa.h (28 rows of
  *                        `capacity` doubles, row k at k * capacity), here a
- *                        std::vector
+ *                        std::vector over page-locked memory (mpm_host_alloc)
  *   GPU_Implementation6  gpu_implementation6.h:24-59 for one partition: the
  *                        halo and point-transfer methods do nothing
  *   Model3D              model_3d.h:30-55 / model_3d.cpp:24-112: Reset,
@@ -20,6 +20,7 @@
 #define ICEMPM_B200_HPP
 
 #include <algorithm>
+#include <cstddef>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -35,9 +36,29 @@ inline void check(int code, const char* where) {
     throw std::runtime_error(msg);
 }
 
+// Page-locked host memory from the library (mpm_host_alloc), as
+// HostSideSOA::Allocate takes it with cudaMallocHost (host_side_soa.cpp:70-86).
+template <class T>
+struct PinnedAllocator {
+    using value_type = T;
+    PinnedAllocator() = default;
+    template <class U>
+    PinnedAllocator(const PinnedAllocator<U>&) {}
+    T* allocate(std::size_t count) {
+        void* p = nullptr;
+        check(mpm_host_alloc(count * sizeof(T), &p), "mpm_host_alloc");
+        return static_cast<T*>(p);
+    }
+    void deallocate(T* p, std::size_t) noexcept { mpm_host_free(p); }
+    template <class U>
+    bool operator==(const PinnedAllocator<U>&) const { return true; }
+    template <class U>
+    bool operator!=(const PinnedAllocator<U>&) const { return false; }
+};
+
 // HostSideSOA (host_side_soa.h): 28 rows of `capacity` doubles.
 struct HostSideSOA {
-    std::vector<double> host_buffer;
+    std::vector<double, PinnedAllocator<double>> host_buffer;
     unsigned capacity = 0;
     unsigned size = 0;
 
