@@ -331,11 +331,12 @@ __device__ __forceinline__ void g2p_gather(const DevParams& P, const double* __r
     }
 }
 
-// The particle update after the gather (mpm_kernels.cuh:307-327).
-template <class K>
-__device__ __forceinline__ void g2p_advance(const DevParams& P, double pos[3], const double vel[3],
-                                            const double C[3][3], double F[3][3], double& Jp_inv, long long& util,
-                                            double p0, double& p_tr, double& q_tr) {
+// The particle update after the gather (mpm_kernels.cuh:307-327) up to the
+// failure test: returns true for a crushed solid point, whose return map (on
+// the trial F) is left to k_return_map_f64.
+__device__ __forceinline__ bool g2p_advance_trial(const DevParams& P, double pos[3], const double vel[3],
+                                                  const double C[3][3], double F[3][3], double& Jp_inv,
+                                                  long long& util, double& p_tr, double& q_tr) {
     const double dt = P.dt;
 #pragma unroll
     for (int d = 0; d < 3; d++) pos[d] += vel[d] * dt;
@@ -357,21 +358,27 @@ __device__ __forceinline__ void g2p_advance(const DevParams& P, double pos[3], c
     q_tr = 0;
     if (util & kLiquid) {
         Jp_inv *= det3(A);
-        return;
+        return false;
     }
     double Je;
     trial_pq(P, F, Je, p_tr, q_tr);
     if (!(util & kCrushed)) {
         if (outside_failure_surface(P, (short)util, p_tr, q_tr)) util |= kCrushed;
     }
-    if (util & kCrushed) drucker_prager_return<K>(P, F, Jp_inv, Je, p_tr, q_tr, p0);
+    return (util & kCrushed) != 0;
 }
 
-// partition_kernel_g2p without migration (mpm_kernels.cuh:237-351).
+// partition_kernel_g2p without migration (mpm_kernels.cuh:237-351), up to
+// the failure test; a crushed point is appended to rm_list and its return map
+// runs in k_return_map_f64 (it needs the SVD, whose registers would hold every
+// thread of this kernel). 7 blocks of 128 per SM at 72 registers: 0.80 ms per
+// launch on the 8 M block against 0.90 ms with the return map inline at 128
+// registers (5 blocks: 0.90, 6: 0.85, 8 at 64 registers: 0.83 ms).
+constexpr int kG2PF64Blocks = 7;
 template <class K>
-__global__ void __launch_bounds__(128, 4) k_g2p_f64(DevParams P, double* __restrict__ pts, size_t pitch, int n,
-                                                 const double* __restrict__ grid, int record_pq,
-                                                 const double* __restrict__ p0_arr, int* err) {
+__global__ void __launch_bounds__(128, kG2PF64Blocks) k_g2p_f64(DevParams P, double* __restrict__ pts, size_t pitch,
+                                                 int n, const double* __restrict__ grid, int record_pq,
+                                                 int* err, int* __restrict__ rm_list, int* __restrict__ rm_count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     long long util = __double_as_longlong(pts[i]);
@@ -384,12 +391,11 @@ __global__ void __launch_bounds__(128, 4) k_g2p_f64(DevParams P, double* __restr
 #pragma unroll
         for (int c = 0; c < 3; c++) F[r][c] = pts[(MPM_FE00 + 3 * r + c) * pitch + i];
     double Jp_inv = pts[MPM_IDX_JP_INV * pitch + i];
-    const double p0 = p0_arr ? p0_arr[i] : P.p0;
 
     double vel[3], C[3][3];
     g2p_gather(P, grid, pos, vel, C, err);
     double p_tr, q_tr;
-    g2p_advance<K>(P, pos, vel, C, F, Jp_inv, util, p0, p_tr, q_tr);
+    if (g2p_advance_trial(P, pos, vel, C, F, Jp_inv, util, p_tr, q_tr)) rm_list[atomicAdd(rm_count, 1)] = i;
 
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -408,6 +414,37 @@ __global__ void __launch_bounds__(128, 4) k_g2p_f64(DevParams P, double* __restr
     if (record_pq) {
         pts[MPM_IDX_P * pitch + i] = p_tr;
         pts[MPM_IDX_Q * pitch + i] = q_tr;
+    }
+}
+
+// The return map (mpm_kernels.cuh:494-544) of the points k_g2p_f64 listed:
+// the trial p, q again from the stored trial F (the same arithmetic), then
+// F and Jp_inv projected. The list holds *count indices; the kernel also
+// clears next_count, the counter the next k_g2p_f64 appends to.
+template <class K>
+__global__ void __launch_bounds__(128) k_return_map_f64(DevParams P, double* __restrict__ pts, size_t pitch,
+                                                        const double* __restrict__ p0_arr,
+                                                        const int* __restrict__ rm_list, const int* __restrict__ count,
+                                                        int* __restrict__ next_count) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *next_count = 0;
+    const int m = *count;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const int i = rm_list[k];
+        double F[3][3];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) F[r][c] = pts[(MPM_FE00 + 3 * r + c) * pitch + i];
+        double Jp_inv = pts[MPM_IDX_JP_INV * pitch + i];
+        const double p0 = p0_arr ? p0_arr[i] : P.p0;
+        double Je, p_tr, q_tr;
+        trial_pq(P, F, Je, p_tr, q_tr);
+        drucker_prager_return<K>(P, F, Jp_inv, Je, p_tr, q_tr, p0);
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) pts[(MPM_FE00 + 3 * r + c) * pitch + i] = F[r][c];
+        pts[MPM_IDX_JP_INV * pitch + i] = Jp_inv;
     }
 }
 

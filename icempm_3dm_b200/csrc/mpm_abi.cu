@@ -392,10 +392,20 @@ int launch_g2p(mpm_handle* h, int record_pq) {
         return r ? r : launch_return_map_mixed(h, 0);
     }
     const unsigned nb = blocks_for(n, 128);
-    if (h->precision == MPM_PRECISION_FP64)
-        k_g2p_f64<SvdF32><<<nb, 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, record_pq, h->p0, h->err);
-    else
-        k_g2p_f64<SvdF64><<<nb, 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, record_pq, h->p0, h->err);
+    const int cur = h->rm_parity;
+    h->rm_parity ^= 1;
+    int* const cnt = h->rm_counts + cur;
+    int* const next = h->rm_counts + (cur ^ 1);
+    const int rb = h->num_sms * 4;
+    if (h->precision == MPM_PRECISION_FP64) {
+        k_g2p_f64<SvdF32><<<nb, 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, record_pq, h->err,
+                                                    h->rm_list, cnt);
+        k_return_map_f64<SvdF32><<<rb, 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, h->p0, h->rm_list, cnt, next);
+    } else {
+        k_g2p_f64<SvdF64><<<nb, 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, n, h->grid, record_pq, h->err,
+                                                    h->rm_list, cnt);
+        k_return_map_f64<SvdF64><<<rb, 128, 0, h->stream>>>(h->dp, h->pts, h->pitch, h->p0, h->rm_list, cnt, next);
+    }
     CK_LAUNCH(h, "g2p kernel");
     return MPM_OK;
 }
@@ -591,16 +601,19 @@ mpm_handle* mpm_create(const SimParams3D* prms, int precision, unsigned capacity
             st = MPM_ERR_CUDA;
             break;
         }
+        if (cudaMalloc(&h->rm_list, sizeof(int) * h->pitch) != cudaSuccess ||
+            cudaMalloc(&h->rm_counts, sizeof(int) * 2) != cudaSuccess) {
+            st = MPM_ERR_CUDA;
+            break;
+        }
+        cudaMemsetAsync(h->rm_counts, 0, sizeof(int) * 2, h->stream);
         if (precision == MPM_PRECISION_MIXED) {
             if (cudaMalloc(&h->mx, sizeof(float) * MPM_N_PTS_ARRAYS * h->pitch) != cudaSuccess ||
                 cudaMalloc(&h->gacc, sizeof(float4) * (size_t)h->dp.nodes) != cudaSuccess ||
-                cudaMalloc(&h->gvel, sizeof(float4) * (size_t)h->dp.nodes) != cudaSuccess ||
-                cudaMalloc(&h->rm_list, sizeof(int) * h->pitch) != cudaSuccess ||
-                cudaMalloc(&h->rm_counts, sizeof(int) * 2) != cudaSuccess) {
+                cudaMalloc(&h->gvel, sizeof(float4) * (size_t)h->dp.nodes) != cudaSuccess) {
                 st = MPM_ERR_CUDA;
                 break;
             }
-            cudaMemsetAsync(h->rm_counts, 0, sizeof(int) * 2, h->stream);
             cudaMemsetAsync(h->mx, 0, sizeof(float) * MPM_N_PTS_ARRAYS * h->pitch, h->stream);
             cudaMemsetAsync(h->gacc, 0, sizeof(float4) * (size_t)h->dp.nodes, h->stream);
             cudaMemsetAsync(h->gvel, 0, sizeof(float4) * (size_t)h->dp.nodes, h->stream);
