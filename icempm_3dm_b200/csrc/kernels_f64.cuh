@@ -167,78 +167,103 @@ __global__ void __launch_bounds__(128, 6) k_p2g_pairs_f64(DevParams P, const dou
 // v = mv/m, gravity, speed clamp, cylindrical indenter contact with its force
 // added to the angle x z sensor and to this substep's total, wall conditions.
 // force3 receives the block-reduced force of this substep (3 doubles).
+// One node with mass of partition_kernel_update_nodes: v (the node's momentum
+// on entry) becomes its velocity; the contact force goes to f and the sensor.
+__device__ __forceinline__ void update_node_f64(const DevParams& P, double* __restrict__ grid, long long idx,
+                                                double mass, double v[3], double ind_x, double ind_y,
+                                                double* __restrict__ sensor, double f[3]) {
+    int idx_z, idx_y;
+    const long long col = div_by64(idx, P.Gz, P.inv_gz, idx_z);
+    const int idx_x = (int)div_by64(col, P.Gy, P.inv_gy, idx_y);
+    const int gx = idx_x - P.halo, gy = idx_y, gz = idx_z;
+#pragma unroll
+    for (int k = 0; k < 3; k++) v[k] /= mass;
+    v[1] -= P.dt_gravity;
+    const double vsq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    if (vsq > P.vmax_sq) {
+        const double nv = sqrt(vsq);
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[k] = v[k] / nv * P.vmax;
+    }
+    if (P.setup_type != 2) {
+        double n0 = gx * P.h - ind_x, n1 = gy * P.h - ind_y;
+        const double nsq = n0 * n0 + n1 * n1;
+        if (nsq < P.ind_rsq) {
+            const double vrel[3] = {v[0] - P.ind_velocity, v[1], v[2]};
+            if (nsq > 0) { const double nn = sqrt(nsq); n0 /= nn; n1 /= nn; }
+            const double vn = vrel[0] * n0 + vrel[1] * n1;
+            if (vn < 0) {
+                const double vt[3] = {vrel[0] - n0 * vn, vrel[1] - n1 * vn, vrel[2]};
+                const double prev[3] = {v[0], v[1], v[2]};
+                v[0] = P.ind_velocity + vt[0];
+                v[1] = vt[1];
+                v[2] = vt[2];
+                // a node in the overlap of two partitions is updated
+                // by both; its force is counted by its owner only
+                if (gx >= P.own_lo && gx < P.own_hi) {
+                    double fn[3];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) { fn[k] = (prev[k] - v[k]) * mass / P.dt; f[k] += fn[k]; }
+                    float angle = atan2f((float)n0, (float)n1);
+                    angle = (float)((double)angle + MPM_PI);
+                    angle = (float)((double)angle * (P.subdiv / (2 * MPM_PI)));
+                    const int ia = min(max((int)angle, 0), P.subdiv - 1);
+                    const int iz = min(max(idx_z, 0), P.Gz - 1);
+                    double* s = sensor + 3 * (iz + ia * P.Gz);
+                    atomicAdd(s + 0, fn[0]);
+                    atomicAdd(s + 1, fn[1]);
+                    atomicAdd(s + 2, fn[2]);
+                }
+            }
+        }
+    }
+    if (P.setup_type != 2) {
+        if (gy <= 2) { v[0] = v[1] = v[2] = 0; }
+    } else {
+        if (gy <= 2 && v[1] < 0) v[1] = 0;
+    }
+    if (gy >= P.Gy - 3 && v[1] > 0) v[1] = 0;
+    if (gx <= 2 && v[0] < 0) v[0] = 0;
+    else if (gx >= P.Gx - 3 && v[0] > 0) v[0] = 0;
+    if (gz <= 2 && v[2] < 0) v[2] = 0;
+    else if (gz >= P.Gz - 3 && v[2] > 0) v[2] = 0;
+    if (P.setup_type == 2 && P.drag != 0) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[k] *= (1 - P.drag);
+    }
+    grid[P.gstride + idx] = v[0];
+    grid[2 * P.gstride + idx] = v[1];
+    grid[3 * P.gstride + idx] = v[2];
+}
+
+// partition_kernel_update_nodes (mpm_kernels.cuh:138-232) for one partition:
+// v = mv/m, gravity, speed clamp, cylindrical indenter contact with its force
+// added to the angle x z sensor and to this substep's total, wall conditions.
+// force3 receives the block-reduced force of this substep (3 doubles). Two
+// nodes per thread, BLOCK apart, with all eight of their sums loaded before
+// either is used (8 M block: 0.053 ms against 0.073 ms for one node per thread
+// that read a node's momentum only after its mass).
+constexpr int kUpdateF64NodesPerThread = 2;
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_update_f64(DevParams P, double* __restrict__ grid, double ind_x, double ind_y,
                                                       double* __restrict__ sensor, double* __restrict__ force3) {
-    const long long idx = (long long)P.node_lo + (long long)blockIdx.x * BLOCK + threadIdx.x;
+    constexpr int NPT = kUpdateF64NodesPerThread;
+    const long long idx0 = (long long)P.node_lo + (long long)blockIdx.x * (BLOCK * NPT) + threadIdx.x;
     double f[3] = {0, 0, 0};
-    if (idx < P.node_hi) {
-        const double mass = grid[idx];
-        if (mass != 0) {
-            double v[3] = {grid[P.gstride + idx], grid[2 * P.gstride + idx], grid[3 * P.gstride + idx]};
-            int idx_z, idx_y;
-            const long long col = div_by64(idx, P.Gz, P.inv_gz, idx_z);
-            const int idx_x = (int)div_by64(col, P.Gy, P.inv_gy, idx_y);
-            const int gx = idx_x - P.halo, gy = idx_y, gz = idx_z;
+    double m[NPT], v[NPT][3];
 #pragma unroll
-            for (int k = 0; k < 3; k++) v[k] /= mass;
-            v[1] -= P.dt_gravity;
-            const double vsq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-            if (vsq > P.vmax_sq) {
-                const double nv = sqrt(vsq);
+    for (int j = 0; j < NPT; j++) {
+        const long long idx = idx0 + j * BLOCK;
+        m[j] = 0;
+        if (idx < P.node_hi) {
+            m[j] = grid[idx];
 #pragma unroll
-                for (int k = 0; k < 3; k++) v[k] = v[k] / nv * P.vmax;
-            }
-            if (P.setup_type != 2) {
-                double n0 = gx * P.h - ind_x, n1 = gy * P.h - ind_y;
-                const double nsq = n0 * n0 + n1 * n1;
-                if (nsq < P.ind_rsq) {
-                    const double vrel[3] = {v[0] - P.ind_velocity, v[1], v[2]};
-                    if (nsq > 0) { const double nn = sqrt(nsq); n0 /= nn; n1 /= nn; }
-                    const double vn = vrel[0] * n0 + vrel[1] * n1;
-                    if (vn < 0) {
-                        const double vt[3] = {vrel[0] - n0 * vn, vrel[1] - n1 * vn, vrel[2]};
-                        const double prev[3] = {v[0], v[1], v[2]};
-                        v[0] = P.ind_velocity + vt[0];
-                        v[1] = vt[1];
-                        v[2] = vt[2];
-                        // a node in the overlap of two partitions is updated
-                        // by both; its force is counted by its owner only
-                        if (gx >= P.own_lo && gx < P.own_hi) {
-#pragma unroll
-                            for (int k = 0; k < 3; k++) f[k] = (prev[k] - v[k]) * mass / P.dt;
-                            float angle = atan2f((float)n0, (float)n1);
-                            angle = (float)((double)angle + MPM_PI);
-                            angle = (float)((double)angle * (P.subdiv / (2 * MPM_PI)));
-                            const int ia = min(max((int)angle, 0), P.subdiv - 1);
-                            const int iz = min(max(idx_z, 0), P.Gz - 1);
-                            double* s = sensor + 3 * (iz + ia * P.Gz);
-                            atomicAdd(s + 0, f[0]);
-                            atomicAdd(s + 1, f[1]);
-                            atomicAdd(s + 2, f[2]);
-                        }
-                    }
-                }
-            }
-            if (P.setup_type != 2) {
-                if (gy <= 2) { v[0] = v[1] = v[2] = 0; }
-            } else {
-                if (gy <= 2 && v[1] < 0) v[1] = 0;
-            }
-            if (gy >= P.Gy - 3 && v[1] > 0) v[1] = 0;
-            if (gx <= 2 && v[0] < 0) v[0] = 0;
-            else if (gx >= P.Gx - 3 && v[0] > 0) v[0] = 0;
-            if (gz <= 2 && v[2] < 0) v[2] = 0;
-            else if (gz >= P.Gz - 3 && v[2] > 0) v[2] = 0;
-            if (P.setup_type == 2 && P.drag != 0) {
-#pragma unroll
-                for (int k = 0; k < 3; k++) v[k] *= (1 - P.drag);
-            }
-            grid[P.gstride + idx] = v[0];
-            grid[2 * P.gstride + idx] = v[1];
-            grid[3 * P.gstride + idx] = v[2];
+            for (int k = 0; k < 3; k++) v[j][k] = grid[(k + 1) * P.gstride + idx];
         }
     }
+#pragma unroll
+    for (int j = 0; j < NPT; j++)
+        if (m[j] != 0) update_node_f64(P, grid, idx0 + j * BLOCK, m[j], v[j], ind_x, ind_y, sensor, f);
     // block reduction of the substep force (only blocks that touch the
     // indenter contribute non-zero values)
     __shared__ double red[3][BLOCK / 32];

@@ -327,8 +327,7 @@ int launch_p2g(mpm_handle* h) {
 }
 
 int launch_update(mpm_handle* h, double ind_x, double ind_y, double* force3) {
-    // the nodes of the partition's window (one partition: the whole grid)
-    const unsigned nb = blocks_for((long long)h->dp.node_hi - h->dp.node_lo, 256);
+    // the nodes of the partition's window (one partition: the whole grid), two per thread
     if (is_mixed(h)) {
         const unsigned nbm = blocks_for((long long)h->dp.node_hi - h->dp.node_lo, 256 * kUpdateNodesPerThread);
         if (h->gacc_q)
@@ -340,7 +339,9 @@ int launch_update(mpm_handle* h, double ind_x, double ind_y, double* force3) {
         CK_LAUNCH(h, "update mixed");
         return MPM_OK;
     }
-    k_update_f64<256><<<nb, 256, 0, h->stream>>>(h->dp, h->grid, ind_x, ind_y, h->sensor, force3);
+    k_update_f64<256><<<blocks_for((long long)h->dp.node_hi - h->dp.node_lo, 256 * kUpdateF64NodesPerThread), 256, 0,
+                         h->stream>>>(
+        h->dp, h->grid, ind_x, ind_y, h->sensor, force3);
     CK_LAUNCH(h, "update kernel");
     return MPM_OK;
 }
