@@ -680,7 +680,7 @@ def run_io(args):
         buf[:, :m] = down
         f_snap = clock("save_snapshot", lambda: snap.save_snapshot(out_dir, 3, p, buf, m, sens, compress=False))
         _, back, size, _ = clock("read_snapshot", lambda: snap.read_snapshot(f_snap))
-        c = h.cohesion()
+        c = h.cohesion() if coh is not None else None    # blocks without per-particle cohesion
         clock("upload", lambda: h.upload(np.ascontiguousarray(back[:, :size]), cohesion=c))
         host[:, :size] = back[:, :size]
         clock("upload_pinned", lambda: h.upload(host[:, :size] if size == n else
