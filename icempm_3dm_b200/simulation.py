@@ -276,10 +276,14 @@ def pinned_empty(shape, dtype=np.float64):
         return np.empty(shape, dtype=dtype)
     ptr = ctypes.c_void_p()
     check(LIB.mpm_host_alloc(nbytes, ctypes.byref(ptr)), "mpm_host_alloc")
+    free = LIB.mpm_host_free          # bound now: module globals may be gone when the last view dies
 
     class PinnedBytes(ctypes.c_char * nbytes):
         def __del__(self):
-            LIB.mpm_host_free(ctypes.c_void_p(ctypes.addressof(self)))
+            try:
+                free(ctypes.c_void_p(ctypes.addressof(self)))
+            except Exception:         # interpreter shutdown: the process returns the memory
+                pass
 
     return np.frombuffer(PinnedBytes.from_address(ptr.value), dtype=dtype).reshape(shape)
 
